@@ -1,0 +1,176 @@
+"""Generate the golden fixtures in ``tests/golden/`` by running the reference
+(DALIA, pure Python) in this container on seeded synthetic problems.
+
+Usage (needs the reference checkout; it is not needed to *use* the fixtures)::
+
+    ARRAY_MODULE=numpy python tests/golden/make_golden.py /path/to/DALIA
+
+For every case the reference's own classes are driven end to end:
+
+* ``Model.construct_Q_prior`` / ``construct_Q_conditional`` -> the sparse
+  precision matrices (COO triplets are stored);
+* ``DenseSolver`` (exact LAPACK, ``src/dalia/solvers/dense_solver.py``):
+  log-determinant, solution, full inverse restricted to the BTA pattern,
+  marginal variances, ``f(theta)`` and the central-FD gradient via
+  ``DALIA._objective_function``;
+* ``SerinvSolver`` with ``serinv.algs`` provided by ``oracle.bta_ref`` (Serinv
+  itself is not installable here): ``f(theta)`` and gradient.  For the Poisson
+  case the solver's ``cholesky`` gets ``sparsity="bta"`` as default, because
+  the reference calls it without that argument (``src/dalia/core/dalia.py:1058``).
+
+The dense path pins the oracle; the Serinv path pins the oracle's restatement
+of DALIA's driver logic (including the prior log-determinant quirk: ``"bt"``
+drops the fixed-effect tip).
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+
+CASES = {
+    # name: (ns, nt, nb, no, theta, likelihood, seed, store_selinv)
+    "gst_small": (48, 4, 3, 40, (-1.0, 1.0, 0.0, 2.0), "gaussian", 1, True),
+    "gst_ragged": (70, 3, 2, 50, (-0.5, 0.7, 0.2, 1.5), "gaussian", 2, True),
+    "pst_small": (40, 4, 2, 60, (-1.2, 0.8, -0.3), "poisson", 3, False),
+    "gst_300x10": (300, 10, 4, 200, (-1.0, 1.0, 0.0, 2.0), "gaussian", 0, False),
+}
+
+
+def checksums(prob):
+    out = {}
+    for nm in ("c0", "g1", "g2", "g3", "m0", "m1", "m2", "a_st"):
+        d = getattr(prob, nm).tocsc().data
+        out[nm] = np.array([d.sum(), (d * d).sum(), d.size], dtype=np.float64)
+    out["a_fe"] = np.array([prob.a_fe.sum(), (prob.a_fe ** 2).sum(), prob.a_fe.size])
+    out["y"] = np.array([prob.y.sum(), (prob.y ** 2).sum(), prob.y.size])
+    return out
+
+
+def main(ref_root: str) -> None:
+    os.environ.setdefault("ARRAY_MODULE", "numpy")
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, os.path.join(ref_root, "src"))
+
+    from oracle import bta_ref
+
+    fake = types.ModuleType("serinv")
+    algs = types.ModuleType("serinv.algs")
+    for nm in ("pobtaf", "pobtas", "pobtasi", "pobtf", "pobts", "pobtsi"):
+        setattr(algs, nm, getattr(bta_ref, nm))
+    fake.algs = algs
+    sys.modules["serinv"] = fake
+    sys.modules["serinv.algs"] = algs
+
+    from dalia.configs import dalia_config, likelihood_config, submodels_config
+    from dalia.core.dalia import DALIA
+    from dalia.core.model import Model
+    from dalia.solvers.structured_solver import SerinvSolver
+    from dalia.submodels import RegressionSubModel, SpatioTemporalSubModel
+
+    from dalia_b200 import synth
+
+    _orig_chol = SerinvSolver.cholesky
+
+    def _chol_default(self, A, sparsity="bta"):
+        return _orig_chol(self, A, sparsity)
+
+    SerinvSolver.cholesky = _chol_default
+
+    for name, (ns, nt, nb, no, theta, lik, seed, store_selinv) in CASES.items():
+        prob = synth.make_problem(ns, nt, nb, no, theta, lik, seed=seed)
+        tmp = tempfile.mkdtemp(prefix=f"golden_{name}_")
+        synth.save_dalia_layout(prob, tmp)
+
+        def build(solver_type):
+            st = SpatioTemporalSubModel(config=submodels_config.parse_config({
+                "type": "spatio_temporal",
+                "input_dir": f"{tmp}/inputs_spatio_temporal",
+                "spatial_domain_dimension": 2,
+                "r_s": theta[0], "r_t": theta[1], "sigma_st": theta[2],
+                "manifold": "plane",
+                "ph_s": {"type": "penalized_complexity", "alpha": 0.01, "u": 0.5},
+                "ph_t": {"type": "penalized_complexity", "alpha": 0.01, "u": 5},
+                "ph_st": {"type": "penalized_complexity", "alpha": 0.01, "u": 3},
+            }))
+            rg = RegressionSubModel(config=submodels_config.parse_config({
+                "type": "regression",
+                "input_dir": f"{tmp}/inputs_regression",
+                "n_fixed_effects": nb,
+                "fixed_effects_prior_precision": 0.001,
+            }))
+            if lik == "gaussian":
+                ld = {"type": "gaussian", "prec_o": theta[3],
+                      "prior_hyperparameters": {"type": "penalized_complexity", "alpha": 0.01, "u": 4}}
+            else:
+                ld = {"type": "poisson", "input_dir": tmp}
+            model = Model(submodels=[rg, st], likelihood_config=likelihood_config.parse_config(ld))
+            dal = DALIA(model=model, config=dalia_config.parse_config({
+                "solver": {"type": solver_type},
+                "inner_iteration_max_iter": 50,
+                "eps_inner_iteration": 1e-3,
+                "eps_gradient_f": 1e-3,
+                "simulation_dir": tmp,
+            }))
+            dal.iter = 0
+            return model, dal
+
+        out = {"theta": np.asarray(theta, dtype=np.float64),
+               "shape": np.array([ns, nt, nb, no, seed]),
+               "likelihood": np.array(lik)}
+        for k, v in checksums(prob).items():
+            out[f"chk_{k}"] = v
+
+        # --- dense solver: exact reference numbers
+        model, dal = build("dense")
+        th = np.asarray(theta, dtype=np.float64)
+        model.theta[:] = th
+        Qp = model.construct_Q_prior().tocoo()
+        eta0 = np.zeros_like(model.y)
+        Qc = model.construct_Q_conditional(eta0).tocoo()
+        if lik == "gaussian" and store_selinv:
+            out["qp_row"], out["qp_col"], out["qp_data"] = Qp.row, Qp.col, Qp.data
+            out["qc_row"], out["qc_col"], out["qc_data"] = Qc.row, Qc.col, Qc.data
+        if lik == "gaussian":
+            dal.solver.cholesky(Qc)
+            out["logdet_qc"] = np.array(dal.solver.logdet())
+            rhs = model.construct_information_vector(eta0, np.zeros_like(model.x))
+            out["rhs"] = rhs.copy()
+            out["x_solve"] = dal.solver.solve(rhs.copy()).copy()
+            if store_selinv:
+                Sinv = dal.solver.selected_inversion()
+                D, L, Ab, T = bta_ref.dense_to_bta(np.asarray(Sinv), nt, ns, nb)
+                out["sel_D"], out["sel_L"], out["sel_Ab"], out["sel_T"] = D, L, Ab, T
+        f_d, g_d = dal._objective_function(th.copy())
+        out["f_dense"] = np.array(f_d)
+        out["grad_dense"] = np.asarray(g_d)
+        out["x_dense"] = model.x.copy()
+        if lik == "gaussian":
+            out["marg_var_dense"] = dal.get_marginal_variances_latent_parameters(
+                th.copy(), model.x.copy())
+
+        # --- Serinv solver path (serinv.algs = BTA oracle)
+        model, dal = build("serinv")
+        f_s, g_s = dal._objective_function(th.copy())
+        out["f_serinv"] = np.array(f_s)
+        out["grad_serinv"] = np.asarray(g_s)
+        out["x_serinv"] = model.x.copy()
+        if lik == "gaussian":
+            out["marg_var_serinv"] = dal.get_marginal_variances_latent_parameters(
+                th.copy(), model.x.copy())
+
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        print(f"{name}: f_dense={f_d:.10f} f_serinv={f_s:.10f} "
+              f"diff={f_d - f_s:.6f} grad_serinv={np.asarray(g_s)}", flush=True)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DALIA_REF", "/root/reference"))
