@@ -1,0 +1,435 @@
+// Host orchestration of the BTA factorisation, solve, selected inversion and
+// log-determinant, exported through the C ABI declared in include/dalia_bta.h.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "../../include/dalia_bta.h"
+#include "bta_internal.cuh"
+#include "gemm.cuh"
+#include "panel.cuh"
+
+using namespace bta;
+
+struct bta_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  char* ws = nullptr;
+  size_t ws_bytes = 0;
+  int* ctl = nullptr;  // [0] abort flag, [1] scratch; ctl+2 (8-aligned): info (u64)
+  double* scal = nullptr;
+  std::map<std::tuple<int, int, int>, std::pair<int4*, int>> tasks;
+};
+
+namespace {
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
+
+struct Carve {
+  char* base;
+  size_t off = 0;
+  template <class T_>
+  T_* take(size_t count) {
+    T_* p = reinterpret_cast<T_*>(base + off);
+    off = align_up(off + count * sizeof(T_));
+    return p;
+  }
+};
+
+int ensure_ws(bta_context* h, size_t bytes) {
+  if (bytes <= h->ws_bytes) return BTA_OK;
+  if (h->ws) {
+    cudaStreamSynchronize(h->stream);
+    cudaFree(h->ws);
+    h->ws = nullptr;
+    h->ws_bytes = 0;
+  }
+  size_t want = align_up(bytes + (bytes >> 4));
+  if (cudaMalloc(&h->ws, want) != cudaSuccess) {
+    cudaGetLastError();
+    return BTA_ERR_ALLOC;
+  }
+  h->ws_bytes = want;
+  return BTA_OK;
+}
+
+inline unsigned long long* info_ptr(bta_context* h) { return reinterpret_cast<unsigned long long*>(h->ctl + 2); }
+
+int cuda_rc(cudaError_t e) { return e == cudaSuccess ? BTA_OK : BTA_ERR_CUDA; }
+int cuda_rc(int e) { return e == 0 ? BTA_OK : BTA_ERR_CUDA; }
+
+// Cached device task list of a single-instance panel.
+int get_tasks(bta_context* h, int b, int a, bool hasL, const int4** out, int* count) {
+  auto key = std::make_tuple(b, a, hasL ? 1 : 0);
+  auto it = h->tasks.find(key);
+  if (it == h->tasks.end()) {
+    PanelInst I{};
+    I.b = b;
+    I.a = a;
+    I.nq = (b + 63) / 64;
+    I.L = hasL ? reinterpret_cast<double*>(1) : nullptr;
+    I.nrows_t = panel_rows(b, a, hasL);
+    std::vector<int4> t;
+    panel_tasks({I}, t);
+    int4* d = nullptr;
+    if (cudaMalloc(&d, t.size() * sizeof(int4)) != cudaSuccess) return BTA_ERR_ALLOC;
+    if (cudaMemcpy(d, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess) return BTA_ERR_CUDA;
+    it = h->tasks.emplace(key, std::make_pair(d, (int)t.size())).first;
+  }
+  *out = it->second.first;
+  *count = it->second.second;
+  return BTA_OK;
+}
+
+// Factor one panel (diag block D, optional L below, optional arrow rows Ab).
+int run_panel(bta_context* h, double* D, double* L, double* Ab, int b, int a, long long base, Carve& cv) {
+  const bool hasL = L != nullptr;
+  const int aa = Ab != nullptr ? a : 0;
+  const int nq = (b + 63) / 64;
+  const int nr = panel_rows(b, aa, hasL);
+  double* linv = cv.take<double>((size_t)nq * 64 * 64);
+  int* cnt = cv.take<int>((size_t)2 * nr * nq + 4);
+  const int4* tasks;
+  int ntasks;
+  int rc = get_tasks(h, b, aa, hasL, &tasks, &ntasks);
+  if (rc) return rc;
+  if (cudaMemsetAsync(cnt, 0, ((size_t)2 * nr * nq + 4) * sizeof(int), h->stream) != cudaSuccess) return BTA_ERR_CUDA;
+  PanelBatch B;
+  std::memset(&B, 0, sizeof(B));
+  B.ninst = 1;
+  B.ntasks = ntasks;
+  B.tasks = tasks;
+  B.counter = cnt + 2 * nr * nq;
+  B.abort_flag = h->ctl;
+  PanelInst& I = B.inst[0];
+  I.D = D;
+  I.L = L;
+  I.Ab = aa ? Ab : nullptr;
+  I.Linv = linv;
+  I.upd = cnt;
+  I.flag = cnt + nr * nq;
+  I.info = info_ptr(h);
+  I.pivot_base = base;
+  I.b = b;
+  I.a = aa;
+  I.nq = nq;
+  I.nrows_t = nr;
+  return cuda_rc(panel_launch(B, 0, h->stream));
+}
+
+size_t panel_ws_bytes(int b, int a) {
+  const int nq = (b + 63) / 64;
+  const int nr = panel_rows(b, a, true);
+  return align_up((size_t)nq * 4096 * 8) + align_up(((size_t)2 * nr * nq + 4) * 4) + 2 * kAlign;
+}
+
+int check_status(bta_context* h, int64_t* info) {
+  unsigned long long hinfo = 0;
+  int habort = 0;
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return BTA_ERR_CUDA;
+  if (cudaMemcpy(&hinfo, info_ptr(h), sizeof(hinfo), cudaMemcpyDeviceToHost) != cudaSuccess) return BTA_ERR_CUDA;
+  if (cudaMemcpy(&habort, h->ctl, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return BTA_ERR_CUDA;
+  const bool fail = hinfo != ~0ULL;
+  if (info) *info = fail ? (int64_t)hinfo : 0;
+  if (habort) return BTA_ERR_TIMEOUT;
+  return fail ? BTA_ERR_NOT_SPD : BTA_OK;
+}
+
+__global__ void scatter_coo_kernel(const int64_t* row, const int64_t* col, const double* val, int64_t nnz,
+                                   int64_t n, int64_t b, int64_t a, int bt, double* D, double* L, double* Ab,
+                                   double* T) {
+  const int64_t nb = n * b;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = row[e], c = col[e];
+    const double v = val[e];
+    if (r < nb && c < nb) {
+      const int64_t bi = r / b, bj = c / b;
+      if (bi == bj) D[(bi * b + r % b) * b + c % b] = v;
+      else if (bi == bj + 1) L[(bj * b + r % b) * b + c % b] = v;
+    } else if (!bt && a > 0 && r >= nb && r < nb + a) {
+      if (c < nb) Ab[((c / b) * a + (r - nb)) * b + c % b] = v;
+      else if (c < nb + a) T[(r - nb) * a + (c - nb)] = v;
+    }
+  }
+}
+
+__global__ void gather_coo_kernel(const int64_t* row, const int64_t* col, int64_t nnz, int64_t n, int64_t b,
+                                  int64_t a, int bt, const double* D, const double* L, const double* Ab,
+                                  const double* T, double* out) {
+  const int64_t nb = n * b;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnz; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = row[e], c = col[e];
+    double v = 0.0;
+    if (r < nb && c < nb) {
+      const int64_t bi = r / b, bj = c / b;
+      if (bi == bj) v = D[(bi * b + r % b) * b + c % b];
+      else if (bi == bj + 1) v = L[(bj * b + r % b) * b + c % b];
+    } else if (!bt && a > 0 && r >= nb && r < nb + a) {
+      if (c < nb) v = Ab[((c / b) * a + (r - nb)) * b + c % b];
+      else if (c < nb + a) v = T[(r - nb) * a + (c - nb)];
+    }
+    out[e] = v;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bta_error_string(int code) {
+  switch (code) {
+    case BTA_OK: return "success";
+    case BTA_ERR_INVALID: return "invalid argument";
+    case BTA_ERR_CUDA: return "CUDA error";
+    case BTA_ERR_NOT_SPD: return "matrix is not positive definite";
+    case BTA_ERR_TIMEOUT: return "device-side wait timed out";
+    case BTA_ERR_ALLOC: return "scratch allocation failed";
+    default: return "unknown error";
+  }
+}
+
+int bta_create(bta_handle_t* handle) {
+  if (!handle) return BTA_ERR_INVALID;
+  auto* h = new bta_context();
+  cudaGetDevice(&h->device);
+  if (cudaMalloc(&h->ctl, 64) != cudaSuccess || cudaMalloc(&h->scal, 64) != cudaSuccess) {
+    delete h;
+    return BTA_ERR_ALLOC;
+  }
+  cudaMemset(h->ctl, 0, 64);
+  *handle = h;
+  return BTA_OK;
+}
+
+int bta_destroy(bta_handle_t h) {
+  if (!h) return BTA_ERR_INVALID;
+  cudaStreamSynchronize(h->stream);
+  for (auto& kv : h->tasks) cudaFree(kv.second.first);
+  if (h->ws) cudaFree(h->ws);
+  cudaFree(h->ctl);
+  cudaFree(h->scal);
+  delete h;
+  return BTA_OK;
+}
+
+int bta_set_stream(bta_handle_t h, void* stream) {
+  if (!h) return BTA_ERR_INVALID;
+  h->stream = reinterpret_cast<cudaStream_t>(stream);
+  return BTA_OK;
+}
+
+size_t bta_workspace_bytes(bta_handle_t h) { return h ? h->ws_bytes : 0; }
+
+int bta_pobtaf(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, double* L, double* Ab, double* T,
+               int64_t* info) {
+  if (!h || n < 1 || b < 1 || a < 0 || !D || (n > 1 && !L) || (a > 0 && (!Ab || !T))) return BTA_ERR_INVALID;
+  if (b > 65535 * 64 || a > 4096) return BTA_ERR_INVALID;
+  const size_t need = panel_ws_bytes((int)b, (int)a) + (a > 0 ? panel_ws_bytes((int)a, 0) : 0);
+  int rc = ensure_ws(h, need);
+  if (rc) return rc;
+  cudaStream_t s = h->stream;
+  if (cudaMemsetAsync(h->ctl, 0, 8, s) != cudaSuccess) return BTA_ERR_CUDA;
+  if (cudaMemsetAsync(info_ptr(h), 0xff, 8, s) != cudaSuccess) return BTA_ERR_CUDA;
+  const size_t bb = (size_t)b * b, ab = (size_t)a * b;
+  for (int64_t i = 0; i < n; ++i) {
+    const bool hasL = i < n - 1;
+    double* Di = D + i * bb;
+    double* Li = hasL ? L + i * bb : nullptr;
+    double* Abi = a > 0 ? Ab + i * ab : nullptr;
+    Carve cv{h->ws};
+    rc = run_panel(h, Di, Li, Abi, (int)b, (int)a, (long long)(i * b), cv);
+    if (rc) return rc;
+    std::vector<GemmProb> probs;
+    if (hasL) {
+      GemmProb p = gemm_prob(D + (i + 1) * bb, (int)b, (int)b, (int)b, 1.0, GC_LOWER);
+      gemm_add(p, Li, (int)b, Li, (int)b, (int)b, -1.0, 0);
+      probs.push_back(p);
+    }
+    if (a > 0) {
+      if (hasL) {
+        GemmProb p = gemm_prob(Ab + (i + 1) * ab, (int)b, (int)a, (int)b, 1.0);
+        gemm_add(p, Abi, (int)b, Li, (int)b, (int)b, -1.0, 0);
+        probs.push_back(p);
+      }
+      GemmProb p = gemm_prob(T, (int)a, (int)a, (int)a, 1.0);
+      gemm_add(p, Abi, (int)b, Abi, (int)b, (int)b, -1.0, 0);
+      probs.push_back(p);
+    }
+    if (!probs.empty() && gemm_launch(probs, s) != cudaSuccess) return BTA_ERR_CUDA;
+  }
+  if (a > 0) {
+    Carve cv{h->ws};
+    rc = run_panel(h, T, nullptr, nullptr, (int)a, 0, (long long)(n * b), cv);
+    if (rc) return rc;
+  }
+  if (info) return check_status(h, info);
+  return cuda_rc(cudaGetLastError());
+}
+
+int bta_pobtas(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D, const double* L,
+               const double* Ab, const double* T, double* rhs, int trans) {
+  if (!h || n < 1 || b < 1 || a < 0 || !D || !rhs || (n > 1 && !L) || (a > 0 && (!Ab || !T))) return BTA_ERR_INVALID;
+  if (trans != 0 && trans != 1) return BTA_ERR_INVALID;
+  const int nq = (int)((b + 63) / 64);
+  const size_t need = align_up((size_t)n * nq * 4096 * 8) + align_up(((size_t)n * nq + 4) * 4) + kAlign;
+  int rc = ensure_ws(h, need);
+  if (rc) return rc;
+  cudaStream_t s = h->stream;
+  Carve cv{h->ws};
+  double* tinv = cv.take<double>((size_t)n * nq * 4096);
+  int* flags = cv.take<int>((size_t)n * nq + 4);
+  if (cudaMemsetAsync(flags, 0, ((size_t)n * nq + 4) * sizeof(int), s) != cudaSuccess) return BTA_ERR_CUDA;
+  if (cudaMemsetAsync(h->ctl, 0, 4, s) != cudaSuccess) return BTA_ERR_CUDA;
+  if (diag_tile_inverses(D, (int)n, (int)b, tinv, s)) return BTA_ERR_CUDA;
+  SweepArgs A{};
+  A.D = D;
+  A.L = L;
+  A.Ab = Ab;
+  A.Linv = tinv;
+  A.x = rhs;
+  A.flags = flags;
+  A.counter = flags + n * nq;
+  A.abort_flag = h->ctl;
+  A.n = (int)n;
+  A.b = (int)b;
+  A.a = (int)a;
+  A.nq = nq;
+  A.trans = trans;
+  if (trans == 0) {
+    if (sweep_launch(A, s)) return BTA_ERR_CUDA;
+    if (arrow_forward(Ab, T, rhs, (int)n, (int)b, (int)a, s)) return BTA_ERR_CUDA;
+  } else {
+    if (arrow_backward(T, rhs, (int)n, (int)b, (int)a, s)) return BTA_ERR_CUDA;
+    if (sweep_launch(A, s)) return BTA_ERR_CUDA;
+  }
+  return cuda_rc(cudaGetLastError());
+}
+
+int bta_pobtasi(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, double* L, double* Ab, double* T) {
+  if (!h || n < 1 || b < 1 || a < 0 || !D || (n > 1 && !L) || (a > 0 && (!Ab || !T))) return BTA_ERR_INVALID;
+  const int nq = (int)((b + 63) / 64);
+  const int nqa = (int)((a + 63) / 64);
+  const size_t bb = (size_t)b * b, ab = (size_t)a * b;
+  const size_t need = align_up((size_t)n * nq * 4096 * 8) + align_up((size_t)n * bb * 8) + 2 * align_up(bb * 8) +
+                      align_up(ab * 8 + 8) + align_up((size_t)nqa * 4096 * 8 + 8) + align_up((size_t)a * a * 8 + 8) +
+                      8 * kAlign;
+  int rc = ensure_ws(h, need);
+  if (rc) return rc;
+  cudaStream_t s = h->stream;
+  Carve cv{h->ws};
+  double* tinv = cv.take<double>((size_t)n * nq * 4096);
+  double* Linv = cv.take<double>((size_t)n * bb);
+  double* G = cv.take<double>(bb);
+  double* S = cv.take<double>(bb);
+  double* Ga = cv.take<double>(ab + 1);
+  double* tinv_t = cv.take<double>((size_t)nqa * 4096 + 1);
+  double* Wt = cv.take<double>((size_t)a * a + 1);
+  if (diag_tile_inverses(D, (int)n, (int)b, tinv, s)) return BTA_ERR_CUDA;
+  if (block_trtri(D, tinv, 0, (int)n, (int)b, Linv, s)) return BTA_ERR_CUDA;
+  if (a > 0) {
+    if (diag_tile_inverses(T, 1, (int)a, tinv_t, s)) return BTA_ERR_CUDA;
+    if (block_trtri(T, tinv_t, 0, 1, (int)a, Wt, s)) return BTA_ERR_CUDA;
+    GemmProb p = gemm_prob(T, (int)a, (int)a, (int)a, 0.0, GC_LOWER | GC_MIRROR);
+    gemm_add(p, Wt, (int)a, Wt, (int)a, (int)a, 1.0, GF_A_T | GF_B_KN | GF_K_GE_M | GF_K_GE_N);
+    if (gemm_launch({p}, s)) return BTA_ERR_CUDA;
+  }
+  for (int64_t i = n - 1; i >= 0; --i) {
+    const bool hasL = i < n - 1;
+    double* Di = D + i * bb;
+    double* Li = hasL ? L + i * bb : nullptr;
+    double* Abi = a > 0 ? Ab + i * ab : nullptr;
+    const double* Vi = Linv + i * bb;
+    const int B_ = (int)b, A_ = (int)a;
+    std::vector<GemmProb> pa, pb;
+    if (hasL) {
+      GemmProb p = gemm_prob(G, B_, B_, B_, 0.0);
+      gemm_add(p, Li, B_, Vi, B_, B_, 1.0, GF_B_KN | GF_K_GE_N);
+      pa.push_back(p);
+    }
+    if (a > 0) {
+      GemmProb p = gemm_prob(Ga, B_, A_, B_, 0.0);
+      gemm_add(p, Abi, B_, Vi, B_, B_, 1.0, GF_B_KN | GF_K_GE_N);
+      pa.push_back(p);
+    }
+    if (!pa.empty() && gemm_launch(pa, s)) return BTA_ERR_CUDA;
+    if (hasL) {
+      GemmProb p = gemm_prob(Li, B_, B_, B_, 0.0);
+      gemm_add(p, D + (i + 1) * bb, B_, G, B_, B_, -1.0, GF_B_KN);
+      if (a > 0) gemm_add(p, Ab + (i + 1) * ab, B_, Ga, B_, A_, -1.0, GF_A_T | GF_B_KN);
+      pb.push_back(p);
+    }
+    if (a > 0) {
+      GemmProb p = gemm_prob(Abi, B_, A_, B_, 0.0);
+      if (hasL) gemm_add(p, Ab + (i + 1) * ab, B_, G, B_, B_, -1.0, GF_B_KN);
+      gemm_add(p, T, A_, Ga, B_, A_, -1.0, GF_B_KN);
+      pb.push_back(p);
+    }
+    if (!pb.empty() && gemm_launch(pb, s)) return BTA_ERR_CUDA;
+    GemmProb pc = gemm_prob(S, B_, B_, B_, 0.0, GC_LOWER | GC_MIRROR);
+    gemm_add(pc, Vi, B_, Vi, B_, B_, 1.0, GF_A_T | GF_B_KN | GF_K_GE_M | GF_K_GE_N);
+    if (hasL) gemm_add(pc, G, B_, Li, B_, B_, -1.0, GF_A_T | GF_B_KN);
+    if (a > 0) gemm_add(pc, Ga, B_, Abi, B_, A_, -1.0, GF_A_T | GF_B_KN);
+    if (gemm_launch({pc}, s)) return BTA_ERR_CUDA;
+    if (cudaMemcpyAsync(Di, S, bb * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess) return BTA_ERR_CUDA;
+  }
+  return cuda_rc(cudaGetLastError());
+}
+
+int bta_logdet(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D, const double* T, int include_tip,
+               double* out_device, double* out_host) {
+  if (!h || n < 1 || b < 1 || a < 0 || !D || (include_tip && a > 0 && !T)) return BTA_ERR_INVALID;
+  int rc = ensure_ws(h, align_up((size_t)(n + 2) * 8));
+  if (rc) return rc;
+  double* part = reinterpret_cast<double*>(h->ws);
+  double* out = out_device ? out_device : h->scal;
+  const int at = include_tip ? (int)a : 0;
+  if (logdet_launch(D, (int)n, (int)b, T, at, part, out, h->stream)) return BTA_ERR_CUDA;
+  if (out_host) {
+    if (cudaMemcpyAsync(out_host, out, sizeof(double), cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)
+      return BTA_ERR_CUDA;
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return BTA_ERR_CUDA;
+  }
+  return cuda_rc(cudaGetLastError());
+}
+
+int bta_get_status(bta_handle_t h, int64_t* info) {
+  if (!h) return BTA_ERR_INVALID;
+  return check_status(h, info);
+}
+
+int bta_gather_coo(bta_handle_t h, int64_t n, int64_t b, int64_t a, const int64_t* row, const int64_t* col,
+                   int64_t nnz, int sparsity_bt, const double* D, const double* L, const double* Ab, const double* T,
+                   double* out) {
+  if (!h || n < 1 || b < 1 || a < 0 || !D || (n > 1 && !L) || nnz < 0 || (nnz > 0 && !out)) return BTA_ERR_INVALID;
+  if (!sparsity_bt && a > 0 && (!Ab || !T)) return BTA_ERR_INVALID;
+  if (nnz > 0) {
+    const int grid = (int)std::min<int64_t>((nnz + 255) / 256, 148 * 32);
+    gather_coo_kernel<<<grid, 256, 0, h->stream>>>(row, col, nnz, n, b, a, sparsity_bt, D, L, Ab, T, out);
+  }
+  return cuda_rc(cudaGetLastError());
+}
+
+int bta_scatter_coo(bta_handle_t h, int64_t n, int64_t b, int64_t a, const int64_t* row, const int64_t* col,
+                    const double* val, int64_t nnz, int sparsity_bt, double* D, double* L, double* Ab, double* T) {
+  if (!h || n < 1 || b < 1 || a < 0 || !D || (n > 1 && !L) || nnz < 0) return BTA_ERR_INVALID;
+  if (!sparsity_bt && a > 0 && (!Ab || !T)) return BTA_ERR_INVALID;
+  cudaStream_t s = h->stream;
+  const size_t bb = (size_t)b * b;
+  if (cudaMemsetAsync(D, 0, n * bb * 8, s)) return BTA_ERR_CUDA;
+  if (n > 1 && cudaMemsetAsync(L, 0, (n - 1) * bb * 8, s)) return BTA_ERR_CUDA;
+  if (!sparsity_bt && a > 0) {
+    if (cudaMemsetAsync(Ab, 0, (size_t)n * a * b * 8, s)) return BTA_ERR_CUDA;
+    if (cudaMemsetAsync(T, 0, (size_t)a * a * 8, s)) return BTA_ERR_CUDA;
+  }
+  if (nnz > 0) {
+    const int grid = (int)std::min<int64_t>((nnz + 255) / 256, 148 * 32);
+    scatter_coo_kernel<<<grid, 256, 0, s>>>(row, col, val, nnz, n, b, a, sparsity_bt, D, L, Ab, T);
+  }
+  return cuda_rc(cudaGetLastError());
+}
+
+}  // extern "C"

@@ -1,0 +1,37 @@
+// Internal host-side interfaces between the kernel translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bta {
+
+struct SweepArgs {
+  const double* D;     // n x b x b factor diagonal blocks
+  const double* L;     // (n-1) x b x b factor sub-diagonal blocks
+  const double* Ab;    // n x a x b factor arrow blocks
+  const double* Linv;  // n*nq inverses of the 64x64 diagonal tiles
+  double* x;           // right-hand side in, solution out (n*b + a)
+  int* flags;          // n*nq, zeroed before the launch
+  int* counter;        // zeroed before the launch
+  int* abort_flag;
+  int n, b, a, nq;
+  int trans;  // 0: L y = x,  1: L^T x = y
+};
+
+int diag_tile_inverses(const double* D, int n, int b, double* out, cudaStream_t s);
+int sweep_launch(const SweepArgs& A, cudaStream_t s);
+int arrow_forward(const double* Ab, const double* T, double* x, int n, int b, int a, cudaStream_t s);
+int arrow_backward(const double* T, double* x, int n, int b, int a, cudaStream_t s);
+
+// Full inverses of the lower-triangular factor blocks D[i0..i1) -> out
+// (i1-i0 blocks of b x b, zeros above the diagonal); tile_inv holds the
+// inverses of their diagonal tiles (from diag_tile_inverses, same indexing).
+int block_trtri(const double* D, const double* tile_inv, int i0, int i1, int b, double* out, cudaStream_t s);
+
+// 2 * sum log(diag) over the n diagonal factor blocks (+ the tip when a > 0),
+// written to out (device).  part: n+1 doubles of scratch.
+int logdet_launch(const double* D, int n, int b, const double* T, int a, double* part, double* out,
+                  cudaStream_t s);
+
+}  // namespace bta

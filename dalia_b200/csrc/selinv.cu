@@ -1,0 +1,157 @@
+// Full inverses of the diagonal factor blocks (used by the selected inversion)
+// and the deterministic log-determinant reduction.
+#include <algorithm>
+
+#include "bta_internal.cuh"
+#include "common.cuh"
+#include "tile_ops.cuh"
+
+namespace bta {
+namespace {
+
+using namespace tile;
+constexpr size_t TRTRI_SMEM = size_t(3) * T * SG * sizeof(double);
+
+// One CTA per (block, tile column c): forward substitution down the column,
+//   X[c] = Linv_cc,  X[p] = -Linv_pp * sum_{k=c}^{p-1} L[p][k] X[k]   (p > c).
+// blockIdx.x = c * nblk + block so that the longest columns start first.
+__global__ void __launch_bounds__(THREADS) block_trtri_kernel(const double* D, const double* tile_inv, int i0,
+                                                               int nblk, int b, int nq, double* out) {
+  extern __shared__ __align__(16) double sm[];
+  double* As = sm;
+  double* Bs = sm + T * SG;
+  double* Ys = sm + 2 * T * SG;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t = lane & 3;
+  const int c = blockIdx.x / nblk, bi = blockIdx.x % nblk, i = i0 + bi;
+  const size_t bb = (size_t)b * b;
+  const double* Di = D + (size_t)i * bb;
+  double* Oi = out + (size_t)bi * bb;
+  const int wc = min(T, b - c * T);
+
+  // zero tiles above the diagonal in this column
+  for (int p = 0; p < c; ++p) {
+    for (int idx = tid; idx < T * T; idx += THREADS) {
+      const int r = idx >> 6, cc = idx & 63;
+      if (cc < wc) Oi[(size_t)(p * T + r) * b + c * T + cc] = 0.0;
+    }
+  }
+  // X[c] = Linv_cc
+  {
+    const double* Lc = tile_inv + (size_t)(i * nq + c) * T * T;
+    for (int idx = tid; idx < T * T; idx += THREADS) {
+      const int r = idx >> 6, cc = idx & 63;
+      if (r < wc && cc < wc) Oi[(size_t)(c * T + r) * b + c * T + cc] = Lc[idx];
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  for (int p = c + 1; p < nq; ++p) {
+    const int rp = min(T, b - p * T);
+    double acc[2][4][4];
+    zero_acc(acc);
+    for (int k = c; k < p; ++k) {
+      const int wk = min(T, b - k * T);
+      load<SG>(As, Di + (size_t)(p * T) * b + k * T, b, rp, wk, tid);
+      // Bs[n][j] = X[k][j][n]
+      for (int idx = tid; idx < T * T; idx += THREADS) {
+        const int j = idx >> 6, n = idx & 63;
+        Bs[n * SG + j] = (j < wk && n < wc) ? __ldcg(Oi + (size_t)(k * T + j) * b + c * T + n) : 0.0;
+      }
+      __syncthreads();
+      mma_nt(As, Bs, (wk + 3) & ~3, acc, wm, wn, g, t);
+      __syncthreads();
+    }
+    // Ys[n][j] = acc[j][n]
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int j = wm * 32 + mi * 16 + g + h * 8;
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int n = wn * 32 + ni * 8 + 2 * t + e;
+            Ys[n * SG + j] = acc[mi][ni][h * 2 + e];
+          }
+      }
+    load<SG>(As, tile_inv + (size_t)(i * nq + p) * T * T, T, T, T, tid);
+    __syncthreads();
+    zero_acc(acc);
+    mma_nt(As, Ys, T, acc, wm, wn, g, t);
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int r = wm * 32 + mi * 16 + g + h * 8;
+        if (r >= rp) continue;
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int n = wn * 32 + ni * 8 + 2 * t + e;
+            if (n < wc) Oi[(size_t)(p * T + r) * b + c * T + n] = -acc[mi][ni][h * 2 + e];
+          }
+      }
+    __threadfence();
+    __syncthreads();
+  }
+}
+
+__global__ void logdet_part_kernel(const double* D, int n, int b, const double* Tt, int a, double* part) {
+  __shared__ double red[256];
+  const int blk = blockIdx.x, tid = threadIdx.x;
+  const double* M;
+  int m;
+  if (blk < n) {
+    M = D + (size_t)blk * b * b;
+    m = b;
+  } else {
+    M = Tt;
+    m = a;
+  }
+  double s = 0.0;
+  for (int k = tid; k < m; k += blockDim.x) s += log(M[(size_t)k * m + k]);
+  red[tid] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (tid < o) red[tid] += red[tid + o];
+    __syncthreads();
+  }
+  if (tid == 0) part[blk] = red[0];
+}
+
+__global__ void logdet_final_kernel(const double* part, int cnt, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < cnt; ++i) s += part[i];
+    *out = 2.0 * s;
+  }
+}
+
+}  // namespace
+
+int block_trtri(const double* D, const double* tile_inv, int i0, int i1, int b, double* out, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e =
+        cudaFuncSetAttribute(block_trtri_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRTRI_SMEM);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const int nblk = i1 - i0, nq = (b + T - 1) / T;
+  if (nblk <= 0) return cudaSuccess;
+  block_trtri_kernel<<<nblk * nq, THREADS, TRTRI_SMEM, s>>>(D, tile_inv, i0, nblk, b, nq, out);
+  return cudaGetLastError();
+}
+
+int logdet_launch(const double* D, int n, int b, const double* Tt, int a, double* part, double* out,
+                  cudaStream_t s) {
+  const int cnt = n + (a > 0 ? 1 : 0);
+  if (cnt > 0) logdet_part_kernel<<<cnt, 256, 0, s>>>(D, n, b, Tt, a, part);
+  logdet_final_kernel<<<1, 32, 0, s>>>(part, cnt, out);
+  return cudaGetLastError();
+}
+
+}  // namespace bta

@@ -1,0 +1,291 @@
+// BTA triangular solves (one sweep per call, like Serinv's pobtas) and the
+// batched inverses of the 64x64 diagonal tiles they use.
+//
+// A sweep is one persistent launch over tile rows (block i, tile p) claimed in
+// topological order; each task accumulates its GEMV contributions as the tiles
+// it depends on are published (release/acquire flags, bounded waits) and then
+// applies the inverse of its diagonal tile.
+#include <algorithm>
+
+#include "bta_internal.cuh"
+#include "common.cuh"
+#include "tile_ops.cuh"
+
+namespace bta {
+namespace {
+
+using namespace tile;
+constexpr long long SPIN_LIMIT = 1LL << 24;
+
+__device__ bool wait_flag(const int* p, int* abort_flag) {
+  long long it = 0;
+  while (ld_acquire(p) < 1) {
+    if (ld_acquire(abort_flag)) return false;
+    if (++it > SPIN_LIMIT) {
+      atomicExch(abort_flag, 1);
+      return false;
+    }
+    __nanosleep(64);
+  }
+  return true;
+}
+
+// Inverse of every 64x64 diagonal tile of the n diagonal factor blocks.
+__global__ void __launch_bounds__(THREADS) diag_tile_inverse_kernel(const double* D, int n, int b, int nq,
+                                                                     double* out) {
+  extern __shared__ __align__(16) double sm[];
+  double* S = sm;
+  double* Li = sm + T * SC;
+  const int tid = threadIdx.x;
+  const int i = blockIdx.x / nq, p = blockIdx.x % nq;
+  const int w = min(T, b - p * T);
+  const double* src = D + (size_t)i * b * b + (size_t)(p * T) * b + p * T;
+  load<SC>(S, src, b, w, w, tid);
+  __syncthreads();
+  for (int r = w + tid; r < T; r += THREADS) S[r * SC + r] = 1.0;
+  __syncthreads();
+  trinv(S, Li, tid);
+  double* dst = out + (size_t)blockIdx.x * T * T;
+  for (int idx = tid; idx < T * T; idx += THREADS) {
+    const int r = idx >> 6, c = idx & 63;
+    dst[idx] = (r < w && c < w) ? Li[r * SC + c] : 0.0;
+  }
+}
+
+// acc[r] -= sum_c M[r][c] v[c]  (rows x cols tile, leading dimension ld)
+__device__ __forceinline__ void gemv_sub(const double* M, int ld, int rows, int cols, const double* v,
+                                         double* acc, int tid) {
+  const int lane = tid & 31, warp = tid >> 5;
+  for (int r = warp; r < rows; r += 4) {
+    const double* row = M + (size_t)r * ld;
+    double s = 0.0;
+    if (lane < cols) s += __ldcg(row + lane) * v[lane];
+    if (lane + 32 < cols) s += __ldcg(row + lane + 32) * v[lane + 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) acc[r] -= s;
+  }
+}
+
+// acc[c] -= sum_r M[r][c] v[r]; part is a 128-entry smem scratch.
+__device__ __forceinline__ void gemv_t_sub(const double* M, int ld, int rows, int cols, const double* v,
+                                           double* acc, double* part, int tid) {
+  const int c = tid & 63, half = tid >> 6;
+  double s = 0.0;
+  if (c < cols) {
+    const int r0 = half * 32, r1 = min(rows, r0 + 32);
+    for (int r = r0; r < r1; ++r) s += __ldcg(M + (size_t)r * ld + c) * v[r];
+  }
+  part[tid] = s;
+  __syncthreads();
+  if (tid < 64) acc[tid] -= part[tid] + part[tid + 64];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(THREADS) sweep_kernel(SweepArgs A) {
+  __shared__ double acc[T], v[T], part[2 * T];
+  __shared__ int s_task, s_ok;
+  const int tid = threadIdx.x;
+  const int total = A.n * A.nq;
+  const size_t bb = (size_t)A.b * A.b;
+  for (;;) {
+    if (tid == 0) s_task = atomicAdd(A.counter, 1);
+    __syncthreads();
+    const int ti = s_task;
+    if (ti >= total) break;
+    int i, p;
+    if (A.trans == 0) {
+      i = ti / A.nq;
+      p = ti % A.nq;
+    } else {
+      i = A.n - 1 - ti / A.nq;
+      p = A.nq - 1 - ti % A.nq;
+    }
+    const int rows = min(T, A.b - p * T);
+    double* xi = A.x + (size_t)i * A.b;
+    if (tid < T) acc[tid] = (tid < rows) ? xi[p * T + tid] : 0.0;
+    __syncthreads();
+    bool ok = true;
+    if (A.trans == 0) {
+      if (i > 0) {
+        const double* Lm = A.L + (size_t)(i - 1) * bb + (size_t)(p * T) * A.b;
+        const double* yprev = A.x + (size_t)(i - 1) * A.b;
+        for (int k = 0; k < A.nq && ok; ++k) {
+          if (tid == 0) s_ok = wait_flag(&A.flags[(i - 1) * A.nq + k], A.abort_flag);
+          __syncthreads();
+          ok = s_ok;
+          const int kc = min(T, A.b - k * T);
+          if (ok) {
+            if (tid < T) v[tid] = tid < kc ? __ldcg(yprev + k * T + tid) : 0.0;
+            __syncthreads();
+            gemv_sub(Lm + k * T, A.b, rows, kc, v, acc, tid);
+          }
+          __syncthreads();
+        }
+      }
+      const double* Dm = A.D + (size_t)i * bb + (size_t)(p * T) * A.b;
+      for (int k = 0; k < p && ok; ++k) {
+        if (tid == 0) s_ok = wait_flag(&A.flags[i * A.nq + k], A.abort_flag);
+        __syncthreads();
+        ok = s_ok;
+        if (ok) {
+          if (tid < T) v[tid] = __ldcg(xi + k * T + tid);
+          __syncthreads();
+          gemv_sub(Dm + k * T, A.b, rows, T, v, acc, tid);
+        }
+        __syncthreads();
+      }
+      if (ok) {
+        // y = Linv_pp * acc
+        const double* Li = A.Linv + (size_t)(i * A.nq + p) * T * T;
+        if (tid < T) v[tid] = acc[tid];
+        if (tid < T) acc[tid] = 0.0;
+        __syncthreads();
+        gemv_sub(Li, T, rows, rows, v, acc, tid);
+        __syncthreads();
+        if (tid < rows) xi[p * T + tid] = -acc[tid];
+      }
+    } else {
+      if (A.a > 0) {
+        // acc -= Ab_i[:, p-tile]^T x_a
+        if (tid < T) v[tid] = tid < A.a ? __ldcg(A.x + (size_t)A.n * A.b + tid) : 0.0;
+        __syncthreads();
+        for (int a0 = 0; a0 < A.a; a0 += T) {
+          const int ar = min(T, A.a - a0);
+          if (a0 > 0) {
+            if (tid < T) v[tid] = tid < ar ? __ldcg(A.x + (size_t)A.n * A.b + a0 + tid) : 0.0;
+            __syncthreads();
+          }
+          gemv_t_sub(A.Ab + (size_t)i * A.a * A.b + (size_t)a0 * A.b + p * T, A.b, ar, rows, v, acc, part, tid);
+        }
+      }
+      if (i < A.n - 1) {
+        const double* Lm = A.L + (size_t)i * bb + p * T;
+        const double* xnext = A.x + (size_t)(i + 1) * A.b;
+        for (int k = 0; k < A.nq && ok; ++k) {
+          if (tid == 0) s_ok = wait_flag(&A.flags[(i + 1) * A.nq + k], A.abort_flag);
+          __syncthreads();
+          ok = s_ok;
+          const int kr = min(T, A.b - k * T);
+          if (ok) {
+            if (tid < T) v[tid] = tid < kr ? __ldcg(xnext + k * T + tid) : 0.0;
+            __syncthreads();
+            gemv_t_sub(Lm + (size_t)(k * T) * A.b, A.b, kr, rows, v, acc, part, tid);
+          }
+        }
+      }
+      const double* Dm = A.D + (size_t)i * bb + p * T;
+      for (int k = A.nq - 1; k > p && ok; --k) {
+        if (tid == 0) s_ok = wait_flag(&A.flags[i * A.nq + k], A.abort_flag);
+        __syncthreads();
+        ok = s_ok;
+        const int kr = min(T, A.b - k * T);
+        if (ok) {
+          if (tid < T) v[tid] = tid < kr ? __ldcg(xi + k * T + tid) : 0.0;
+          __syncthreads();
+          gemv_t_sub(Dm + (size_t)(k * T) * A.b, A.b, kr, rows, v, acc, part, tid);
+        }
+      }
+      if (ok) {
+        // x = Linv_pp^T * acc
+        const double* Li = A.Linv + (size_t)(i * A.nq + p) * T * T;
+        if (tid < T) v[tid] = acc[tid];
+        if (tid < T) acc[tid] = 0.0;
+        __syncthreads();
+        gemv_t_sub(Li, T, rows, rows, v, acc, part, tid);
+        if (tid < rows) xi[p * T + tid] = -acc[tid];
+      }
+    }
+    __syncthreads();
+    if (tid == 0 && ok) {
+      __threadfence();
+      st_release(&A.flags[i * A.nq + p], 1);
+    }
+  }
+}
+
+// Forward arrow step: y_a = T^-1 (x_a - sum_i Ab_i y_i); one CTA.
+__global__ void __launch_bounds__(256) arrow_forward_kernel(const double* Ab, const double* Tt, double* x, int n,
+                                                            int b, int a) {
+  extern __shared__ double sa[];  // a values + 256 partials
+  double* ya = sa;
+  double* part = sa + a;
+  const int tid = threadIdx.x;
+  const long long nb = (long long)n * b;
+  for (int r = 0; r < a; ++r) {
+    double s = 0.0;
+    for (long long j = tid; j < nb; j += blockDim.x) {
+      const long long i = j / b, c = j % b;
+      s += Ab[(size_t)i * a * b + (size_t)r * b + c] * x[j];
+    }
+    part[tid] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+      if (tid < o) part[tid] += part[tid + o];
+      __syncthreads();
+    }
+    if (tid == 0) ya[r] = x[nb + r] - part[0];
+    __syncthreads();
+  }
+  if (tid == 0) {
+    for (int r = 0; r < a; ++r) {
+      double s = ya[r];
+      for (int k = 0; k < r; ++k) s -= Tt[r * a + k] * ya[k];
+      ya[r] = s / Tt[r * a + r];
+      x[nb + r] = ya[r];
+    }
+  }
+}
+
+// Backward arrow step: x_a = T^-T y_a (one thread).
+__global__ void arrow_backward_kernel(const double* Tt, double* x, long long nb, int a) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int r = a - 1; r >= 0; --r) {
+    double s = x[nb + r];
+    for (int k = r + 1; k < a; ++k) s -= Tt[k * a + r] * x[nb + k];
+    x[nb + r] = s / Tt[r * a + r];
+  }
+}
+
+}  // namespace
+
+int diag_tile_inverses(const double* D, int n, int b, double* out, cudaStream_t s) {
+  const int nq = (b + T - 1) / T;
+  const size_t smem = size_t(2) * T * SC * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(diag_tile_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  if (n * nq == 0) return cudaSuccess;
+  diag_tile_inverse_kernel<<<n * nq, THREADS, smem, s>>>(D, n, b, nq, out);
+  return cudaGetLastError();
+}
+
+int sweep_launch(const SweepArgs& A, cudaStream_t s) {
+  const int total = A.n * A.nq;
+  if (total == 0) return cudaSuccess;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::min(total, sms * 8);
+  sweep_kernel<<<grid, THREADS, 0, s>>>(A);
+  return cudaGetLastError();
+}
+
+int arrow_forward(const double* Ab, const double* Tt, double* x, int n, int b, int a, cudaStream_t s) {
+  if (a <= 0) return cudaSuccess;
+  const size_t smem = (size_t)(a + 256) * sizeof(double);
+  arrow_forward_kernel<<<1, 256, smem, s>>>(Ab, Tt, x, n, b, a);
+  return cudaGetLastError();
+}
+
+int arrow_backward(const double* Tt, double* x, int n, int b, int a, cudaStream_t s) {
+  if (a <= 0) return cudaSuccess;
+  arrow_backward_kernel<<<1, 32, 0, s>>>(Tt, x, (long long)n * b, a);
+  return cudaGetLastError();
+}
+
+}  // namespace bta

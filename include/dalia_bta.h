@@ -1,0 +1,115 @@
+/*
+ * dalia_bta.h -- C ABI of the B200 block-tridiagonal-arrowhead (BTA) solver.
+ *
+ * Drop-in for the structured-solver path of DALIA (affifboudaoud/DALIA).  The
+ * reference keeps the matrix in four dense FP64 arrays and calls Serinv:
+ *
+ *   D  [n][b][b]   diagonal blocks          (src/dalia/solvers/structured_solver.py:38-41)
+ *   L  [n-1][b][b] sub-diagonal blocks      (structured_solver.py:42-49)
+ *   Ab [n][a][b]   arrow bottom blocks      (structured_solver.py:53-56)
+ *   T  [a][a]      arrow tip                (structured_solver.py:57-60)
+ *
+ * All arrays are C-contiguous row-major FP64 in device memory owned by the
+ * caller; every routine works in place, stream-ordered on the handle's stream.
+ * Return value: BTA_OK or an error code (bta_error_string).  A handle owns only
+ * scratch memory and cached launch plans; use one handle per stream.
+ */
+#ifndef DALIA_BTA_H
+#define DALIA_BTA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BTA_OK 0
+#define BTA_ERR_INVALID 1   /* invalid argument (sizes, null pointers, sparsity) */
+#define BTA_ERR_CUDA 2      /* CUDA runtime error                                 */
+#define BTA_ERR_NOT_SPD 3   /* non-positive pivot: matrix not positive definite   */
+#define BTA_ERR_TIMEOUT 4   /* a bounded device-side wait gave up                 */
+#define BTA_ERR_ALLOC 5     /* scratch allocation failed                          */
+
+typedef struct bta_context* bta_handle_t;
+
+/* Handle life cycle.  The handle binds to the current CUDA device. */
+int bta_create(bta_handle_t* handle);
+int bta_destroy(bta_handle_t handle);
+/* stream: a cudaStream_t (NULL = legacy default stream). */
+int bta_set_stream(bta_handle_t handle, void* stream);
+const char* bta_error_string(int code);
+/* Bytes of scratch currently held by the handle. */
+size_t bta_workspace_bytes(bta_handle_t handle);
+
+/*
+ * In-place BTA Cholesky Q = L L^T.  Replaces Serinv's
+ *   pobtaf(A_diagonal_blocks, A_lower_diagonal_blocks, A_arrow_bottom_blocks, A_arrow_tip_block)
+ * called at src/dalia/solvers/structured_solver.py:83-88.
+ * On exit D holds the lower factors (zeros above the diagonal), L, Ab and T the
+ * factor blocks.  a = 0 gives the BT factorisation (pobtf, :90-93); Ab and T
+ * may then be NULL.  If info != NULL the call synchronises the stream and
+ * writes 0 on success or the 1-based global index of the first non-positive
+ * pivot (then returns BTA_ERR_NOT_SPD).
+ */
+int bta_pobtaf(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, double* L, double* Ab, double* T,
+               int64_t* info);
+
+/*
+ * One triangular sweep with the factor, in place on rhs (length n*b + a).
+ * trans = 0: solve L y = rhs (Serinv trans="N"); trans = 1: solve L^T x = rhs
+ * (trans="C").  Replaces pobtas (structured_solver.py:112-127) and, with a = 0,
+ * pobts (:129-140).
+ */
+int bta_pobtas(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D, const double* L,
+               const double* Ab, const double* T, double* rhs, int trans);
+
+/*
+ * In-place selected inversion of the factor: afterwards D, L, Ab, T hold the
+ * corresponding blocks of Q^{-1} (D full symmetric).  Replaces pobtasi
+ * (structured_solver.py:176-181) and, with a = 0, pobtsi (:183-186).
+ */
+int bta_pobtasi(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, double* L, double* Ab, double* T);
+
+/*
+ * log det Q = 2 (sum_i sum_k log D_i[k][k] + [include_tip] sum_k log T[k][k])
+ * from the factor (SerinvSolver.logdet, structured_solver.py:151-166; the tip
+ * is excluded for sparsity "bt").  out_device (may be NULL) receives the value
+ * stream-ordered; out_host (may be NULL) synchronises and receives it.
+ */
+int bta_logdet(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D, const double* T,
+               int include_tip, double* out_device, double* out_host);
+
+/*
+ * Synchronise the handle's stream and report the status of the last
+ * factorisation: info = 0 or the first non-positive pivot (1-based), return
+ * BTA_ERR_NOT_SPD / BTA_ERR_TIMEOUT accordingly.
+ */
+int bta_get_status(bta_handle_t h, int64_t* info);
+
+/*
+ * Scatter a COO matrix (row, col, val; nnz entries, symmetric storage as
+ * produced by scipy) into zeroed BTA blocks: the device counterpart of
+ * SerinvSolver._spmatrix_to_structured (structured_solver.py:192-390).
+ * Entries outside the BTA pattern are ignored; sparsity_bt != 0 keeps only the
+ * diagonal and sub-diagonal blocks ("bt").
+ */
+int bta_scatter_coo(bta_handle_t h, int64_t n, int64_t b, int64_t a, const int64_t* row, const int64_t* col,
+                    const double* val, int64_t nnz, int sparsity_bt, double* D, double* L, double* Ab,
+                    double* T);
+
+/*
+ * Gather the BTA entries at the COO positions (row, col) into out[nnz]
+ * (zero outside the pattern): the device counterpart of
+ * SerinvSolver._structured_to_spmatrix (structured_solver.py:470-538), which
+ * reads the selected inverse at the lower-triangle pattern of a given matrix.
+ */
+int bta_gather_coo(bta_handle_t h, int64_t n, int64_t b, int64_t a, const int64_t* row, const int64_t* col,
+                   int64_t nnz, int sparsity_bt, const double* D, const double* L, const double* Ab, const double* T,
+                   double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DALIA_BTA_H */

@@ -1,0 +1,123 @@
+"""Parity of the CUDA BTA kernels with the CPU oracle, through the C ABI
+(Serinv-compatible wrappers).  Tolerance: 1e-10 relative (norm-wise), the
+bar the reference's FP64 results are held to."""
+import numpy as np
+import pytest
+
+from golden_util import load, rel
+from oracle import bta_ref
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+SHAPES = [
+    (1, 7, 0), (1, 64, 3), (2, 33, 1), (3, 65, 5), (4, 64, 3), (3, 130, 2),
+    (5, 48, 0), (2, 96, 70), (6, 200, 6), (3, 1, 1), (2, 129, 0),
+]
+
+
+def _cuda(*arrs):
+    import torch
+
+    return [None if a is None else torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in arrs]
+
+
+def _np(*ts):
+    return [None if t is None else t.cpu().numpy() for t in ts]
+
+
+@pytest.mark.parametrize("n,b,a", SHAPES)
+def test_pobtaf_logdet_solve_selinv(n, b, a):
+    from dalia_b200 import serinv_compat as sc
+
+    rng = np.random.default_rng(100 * n + b + a)
+    D, L, Ab, T = bta_ref.random_bta(n, b, a, rng)
+    M = bta_ref.bta_to_dense(D, L, Ab, T)
+    ref = [x.copy() for x in (D, L, Ab, T)]
+    bta_ref.pobtaf(*ref)
+    d = _cuda(D, L, Ab, T)
+    if a == 0:
+        sc.pobtf(d[0], d[1])
+    else:
+        sc.pobtaf(*d)
+    got = _np(*d)
+    assert rel(got[0], ref[0]) < TOL
+    if n > 1:
+        assert rel(got[1], ref[1]) < TOL
+    if a:
+        assert rel(got[2], ref[2]) < TOL and rel(got[3], ref[3]) < TOL
+    # upper triangles of the factor blocks are zero
+    assert np.all(np.triu(got[0], 1) == 0)
+    ld = sc.logdet(d[0], d[3] if a else None, "bta")
+    sign, ld_ref = np.linalg.slogdet(M)
+    assert sign > 0 and abs(ld - ld_ref) < TOL * abs(ld_ref) + 1e-9
+    # solve
+    rhs = rng.standard_normal(n * b + a)
+    x = _cuda(rhs)[0]
+    sc.pobtas(d[0], d[1], d[2] if a else None, d[3] if a else None, x, "N")
+    sc.pobtas(d[0], d[1], d[2] if a else None, d[3] if a else None, x, "C")
+    assert rel(x.cpu().numpy(), np.linalg.solve(M, rhs)) < TOL
+    # selected inversion
+    if a == 0:
+        sc.pobtsi(d[0], d[1])
+    else:
+        sc.pobtasi(*d)
+    got = _np(*d)
+    Sref = bta_ref.dense_to_bta(np.linalg.inv(M), n, b, a)
+    assert rel(got[0], Sref[0]) < TOL
+    if n > 1:
+        assert rel(got[1], Sref[1]) < TOL
+    if a:
+        assert rel(got[2], Sref[2]) < TOL and rel(got[3], Sref[3]) < TOL
+
+
+@pytest.mark.parametrize("name", ["gst_small", "gst_ragged"])
+def test_b200solver_on_reference_precision_matrices(name):
+    """Q_conditional assembled by the reference; results vs the reference's
+    dense LAPACK solver (DenseSolver) stored in the fixture."""
+    import scipy.sparse as sps
+    from dalia_b200.solver import B200Solver
+
+    g = load(name)
+    ns, nt, nb = (int(v) for v in g["shape"][:3])
+    N = ns * nt + nb
+    Qc = sps.coo_matrix((g["qc_data"], (g["qc_row"], g["qc_col"])), shape=(N, N)).tocsc()
+    s = B200Solver(None, diagonal_blocksize=ns, n_diag_blocks=nt, arrowhead_blocksize=nb)
+    s.cholesky(Qc, sparsity="bta")
+    assert abs(s.logdet("bta") - float(g["logdet_qc"])) < TOL * abs(float(g["logdet_qc"]))
+    x = s.solve(g["rhs"].copy(), "bta")
+    assert rel(x, g["x_solve"]) < TOL
+    s.selected_inversion("bta")
+    for k, arr in (("sel_D", s.A_diagonal_blocks), ("sel_L", s.A_lower_diagonal_blocks),
+                   ("sel_Ab", s.A_arrow_bottom_blocks), ("sel_T", s.A_arrow_tip_block)):
+        assert rel(arr.cpu().numpy(), g[k]) < TOL, k
+    mv = s._structured_to_spmatrix(sps.eye(N), "bta").diagonal()
+    assert rel(mv, np.diag(bta_ref.bta_to_dense(g["sel_D"], g["sel_L"], g["sel_Ab"], g["sel_T"]))) < TOL
+
+
+def test_serinv_compat_numpy_host_arrays():
+    from dalia_b200 import serinv_compat as sc
+
+    rng = np.random.default_rng(5)
+    D, L, Ab, T = bta_ref.random_bta(3, 40, 4, rng)
+    ref = [x.copy() for x in (D, L, Ab, T)]
+    bta_ref.pobtaf(*ref)
+    sc.pobtaf(D, L, Ab, T)
+    for g_, r_ in zip((D, L, Ab, T), ref):
+        assert rel(g_, r_) < TOL
+
+
+def test_not_positive_definite_raises():
+    from dalia_b200 import serinv_compat as sc
+
+    rng = np.random.default_rng(7)
+    D, L, Ab, T = bta_ref.random_bta(3, 70, 2, rng)
+    D[1, 5, 5] = -1e6
+    d = _cuda(D, L, Ab, T)
+    with pytest.raises(np.linalg.LinAlgError):
+        sc.pobtaf(*d)
+    # the handle stays usable
+    D2, L2, Ab2, T2 = bta_ref.random_bta(2, 30, 1, rng)
+    d2 = _cuda(D2, L2, Ab2, T2)
+    sc.pobtaf(*d2)
