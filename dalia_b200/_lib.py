@@ -40,10 +40,27 @@ SIGNATURES = {
     "bta_pobtasi": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p]),
     "bta_logdet": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _int, _c_void_p, _pdbl]),
     "bta_get_status": (_int, [_c_void_p, _pi64]),
+    "bta_reset_status": (_int, [_c_void_p]),
     "bta_gather_coo": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _i64, _int,
                               _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p]),
     "bta_scatter_coo": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _i64, _int,
                                _c_void_p, _c_void_p, _c_void_p, _c_void_p]),
+    "bta_assemble_prior": (_int, [_c_void_p, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                  _c_void_p]),
+    "bta_add_entries": (_int, [_c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                               ctypes.c_double, _c_void_p]),
+    "bta_arrow_tip": (_int, [_c_void_p, _i64, _i64, _c_void_p, _c_void_p, ctypes.c_double, ctypes.c_double,
+                             _c_void_p, _int, _c_void_p]),
+    "bta_block_inner": (_int, [_c_void_p, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                               _c_void_p]),
+    "bta_block_quad": (_int, [_c_void_p, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p]),
+    "bta_gather_dot": (_int, [_c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _int, _c_void_p]),
+    "bta_csr_spmv": (_int, [_c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, ctypes.c_double,
+                            ctypes.c_double, _c_void_p]),
+    "bta_symv": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                        _c_void_p]),
+    "bta_dot": (_int, [_c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _int, _c_void_p]),
+    "bta_axpby": (_int, [_c_void_p, _i64, ctypes.c_double, _c_void_p, ctypes.c_double, _c_void_p]),
 }
 
 _lib = None
@@ -134,6 +151,12 @@ def handle(device=None) -> Handle:
     if h is None:
         h = _handles[dev] = Handle(dev)
     return h
+
+
+def stream_ptr(device=None) -> ctypes.c_void_p:
+    import torch
+
+    return _c_void_p(torch.cuda.current_stream(device).cuda_stream)
 
 
 def ptr(t) -> ctypes.c_void_p:

@@ -127,6 +127,12 @@ size_t panel_ws_bytes(int b, int a) {
   return align_up((size_t)nq * 4096 * 8) + align_up(((size_t)2 * nr * nq + 4) * 4) + 2 * kAlign;
 }
 
+int reset_status(bta_context* h) {
+  if (cudaMemsetAsync(h->ctl, 0, 8, h->stream) != cudaSuccess) return BTA_ERR_CUDA;
+  if (cudaMemsetAsync(info_ptr(h), 0xff, 8, h->stream) != cudaSuccess) return BTA_ERR_CUDA;
+  return BTA_OK;
+}
+
 int check_status(bta_context* h, int64_t* info) {
   unsigned long long hinfo = 0;
   int habort = 0;
@@ -201,6 +207,7 @@ int bta_create(bta_handle_t* handle) {
     return BTA_ERR_ALLOC;
   }
   cudaMemset(h->ctl, 0, 64);
+  cudaMemset(info_ptr(h), 0xff, 8);
   *handle = h;
   return BTA_OK;
 }
@@ -232,8 +239,10 @@ int bta_pobtaf(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, doubl
   int rc = ensure_ws(h, need);
   if (rc) return rc;
   cudaStream_t s = h->stream;
-  if (cudaMemsetAsync(h->ctl, 0, 8, s) != cudaSuccess) return BTA_ERR_CUDA;
-  if (cudaMemsetAsync(info_ptr(h), 0xff, 8, s) != cudaSuccess) return BTA_ERR_CUDA;
+  if (info) {
+    rc = reset_status(h);
+    if (rc) return rc;
+  }
   const size_t bb = (size_t)b * b, ab = (size_t)a * b;
   for (int64_t i = 0; i < n; ++i) {
     const bool hasL = i < n - 1;
@@ -283,7 +292,6 @@ int bta_pobtas(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D,
   double* tinv = cv.take<double>((size_t)n * nq * 4096);
   int* flags = cv.take<int>((size_t)n * nq + 4);
   if (cudaMemsetAsync(flags, 0, ((size_t)n * nq + 4) * sizeof(int), s) != cudaSuccess) return BTA_ERR_CUDA;
-  if (cudaMemsetAsync(h->ctl, 0, 4, s) != cudaSuccess) return BTA_ERR_CUDA;
   if (diag_tile_inverses(D, (int)n, (int)b, tinv, s)) return BTA_ERR_CUDA;
   SweepArgs A{};
   A.D = D;
@@ -399,6 +407,11 @@ int bta_logdet(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D,
 int bta_get_status(bta_handle_t h, int64_t* info) {
   if (!h) return BTA_ERR_INVALID;
   return check_status(h, info);
+}
+
+int bta_reset_status(bta_handle_t h) {
+  if (!h) return BTA_ERR_INVALID;
+  return reset_status(h);
 }
 
 int bta_gather_coo(bta_handle_t h, int64_t n, int64_t b, int64_t a, const int64_t* row, const int64_t* col,

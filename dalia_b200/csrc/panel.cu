@@ -9,7 +9,38 @@ namespace bta {
 namespace {
 
 using namespace tile;
-constexpr size_t SMEM_BYTES = size_t(2) * T * SG * sizeof(double) + NPAIR * sizeof(uint16_t) + 64;
+
+#ifdef BTA_TRACE
+// Compile-time task tracer: per event {kind, p, r|q, smid, t_claim, t_ready, t_done}.
+__device__ unsigned long long* g_trace = nullptr;
+__device__ int g_trace_n = 0;
+__device__ __forceinline__ unsigned long long gtime() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void trace(int kind, int p, int rq, unsigned long long t0, unsigned long long t1) {
+  if (threadIdx.x != 0 || g_trace == nullptr) return;
+  const int i = atomicAdd(&g_trace_n, 1);
+  if (i >= (1 << 20)) return;
+  unsigned smid;
+  asm volatile("mov.u32 %0, %smid;" : "=r"(smid));
+  unsigned long long* e = g_trace + (size_t)i * 4;
+  e[0] = ((unsigned long long)kind << 56) | ((unsigned long long)p << 40) | ((unsigned long long)rq << 16) | smid;
+  e[1] = t0;
+  e[2] = t1;
+  e[3] = gtime();
+}
+#define TRACE_T0() unsigned long long _t0 = gtime()
+#define TRACE_T1() unsigned long long _t1 = gtime()
+#define TRACE(kind, p, rq) trace(kind, p, rq, _t0, _t1)
+#else
+#define TRACE_T0()
+#define TRACE_T1()
+#define TRACE(kind, p, rq)
+#endif
+
+constexpr size_t SMEM_BYTES = size_t(2) * T * SG * sizeof(double);
 constexpr long long SPIN_LIMIT = 1LL << 24;
 
 // Bounded wait until *p >= target.  Returns false when the wait gave up.
@@ -21,7 +52,7 @@ __device__ bool wait_ge(const int* p, int target, int* abort_flag) {
       atomicExch(abort_flag, 1);
       return false;
     }
-    __nanosleep(64);
+    __nanosleep(32);
   }
   return true;
 }
@@ -49,33 +80,150 @@ __device__ __forceinline__ TileRef tile_of(const PanelInst& I, int p, int c) {
   return t;
 }
 
-__global__ void __launch_bounds__(THREADS) panel_kernel(const __grid_constant__ PanelBatch B) {
+// Block-wide wait by thread 0; returns the verdict to every thread.
+__device__ __forceinline__ bool block_wait(const int* p, int target, int* abort_flag, int* s_ok) {
+  if (threadIdx.x == 0) *s_ok = wait_ge(p, target, abort_flag) ? 1 : 0;
+  __syncthreads();
+  return *s_ok != 0;
+}
+
+__device__ __forceinline__ void release(int* p, int v) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    st_release(p, v);
+  }
+}
+
+// The critical path of one instance: for q = 0..nq-1,
+//   X = A(q, q-1) Linv_{q-1}^T;  A(q, q) -= X X^T;  POTRF(q);  Linv_q.
+// The two smem buffers swap roles every step: Lv holds Linv_{q-1}, Wk is work.
+__device__ void run_chain(const PanelInst& I, double* bufA, double* bufL, double* rd, int* abort_flag,
+                          int* s_ok) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t = lane & 3;
+  const int nq = I.nq, ld = I.b;
+  double* Lv = bufL;
+  double* Wk = bufA;
+  for (int q = 0; q < nq; ++q) {
+    const TileRef d = tile_of(I, q, q);
+    const int w = d.cols;
+    TRACE_T0();
+    if (q > 0) {
+      if (!block_wait(&I.upd[q * nq + q - 1], q - 1, abort_flag, s_ok)) return;
+      const TileRef x = tile_of(I, q, q - 1);
+      load_async<SG>(Wk, x.ptr, ld, x.rows, x.cols, tid);
+      cp_async_commit();
+      cp_async_wait<0>();
+      __syncthreads();
+      double acc[2][4][4];
+      zero_acc(acc);
+      mma_nt(Wk, Lv, T, acc, wm, wn, g, t);
+      __syncthreads();
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int row = wm * 32 + mi * 16 + g + h * 8;
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int col = wn * 32 + ni * 8 + 2 * t + e;
+              const double v = (row < x.rows) ? acc[mi][ni][h * 2 + e] : 0.0;
+              Wk[row * SG + col] = v;
+              if (row < x.rows && col < x.cols) x.ptr[(size_t)row * ld + col] = v;
+            }
+        }
+      release(&I.flag[q * nq + q - 1], 1);
+      if (!block_wait(&I.upd[q * nq + q], q - 1, abort_flag, s_ok)) return;
+      TRACE_T1();
+      TRACE(8, q, 0);
+      zero_acc(acc);
+      mma_nt(Wk, Wk, T, acc, wm, wn, g, t);
+      // Lv (previous inverse) is dead: it becomes the Cholesky buffer
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int row = wm * 32 + mi * 16 + g + h * 8;
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int col = wn * 32 + ni * 8 + 2 * t + e;
+              double v = 0.0;
+              if (row < w && col < w) v = __ldcg(d.ptr + (size_t)row * ld + col) - acc[mi][ni][h * 2 + e];
+              Lv[row * SG + col] = v;
+            }
+        }
+      __syncthreads();
+    } else {
+      load<SG>(Lv, d.ptr, ld, w, w, tid);
+      __syncthreads();
+    }
+    {
+      TRACE_T0();
+      potrf(Lv, rd, w, I.info, I.pivot_base + (long long)q * T, tid);
+      TRACE_T1();
+      trinv(Lv, Wk, rd, tid);
+      TRACE(9, q, 0);
+    }
+    double* linv = I.Linv + (size_t)q * T * T;
+    for (int idx = tid; idx < T * T; idx += THREADS) {
+      const int i = idx >> 6, k = idx & 63;
+      const bool in = i < w && k < w;
+      if (in) d.ptr[(size_t)i * ld + k] = Lv[i * SG + k];
+      const double li = in ? Wk[i * SG + k] : 0.0;
+      linv[idx] = li;
+      Wk[i * SG + k] = li;  // zero-padded operand for the next step
+    }
+    // strictly-upper tiles of this tile column become zero (LAPACK-style factor)
+    for (int qq = 0; qq < q; ++qq) {
+      double* up = I.D + (size_t)(qq * T) * ld + q * T;
+      for (int idx = tid; idx < T * T; idx += THREADS) {
+        const int i = idx >> 6, k = idx & 63;
+        if (k < w) up[(size_t)i * ld + k] = 0.0;
+      }
+    }
+    double* tmp = Lv;
+    Lv = Wk;
+    Wk = tmp;
+    release(&I.flag[q * nq + q], 1);
+  }
+}
+
+__global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant__ PanelBatch B) {
   extern __shared__ __align__(16) double sm[];
-  double* buf0 = sm;
-  double* buf1 = sm + T * SG;
-  uint16_t* pairs = reinterpret_cast<uint16_t*>(sm + 2 * T * SG);
+  double* bufA = sm;
+  double* bufL = sm + T * SG;
   __shared__ int s_task, s_ok;
-  __shared__ double dg[T];
+  __shared__ double rd[T];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t = lane & 3;
 
-  build_pairs(pairs, tid);
+  // the first CTAs to start take the chain roles (one per instance)
+  if (tid == 0) s_task = atomicAdd(&B.counter[1], 1);
   __syncthreads();
+  if (s_task < B.ninst) {
+    run_chain(B.inst[s_task], bufA, bufL, rd, B.abort_flag, &s_ok);
+    return;
+  }
 
   for (;;) {
-    if (tid == 0) s_task = atomicAdd(B.counter, 1);
+    __syncthreads();
+    if (tid == 0) s_task = atomicAdd(&B.counter[0], 1);
     __syncthreads();
     const int ti = s_task;
     if (ti >= B.ntasks) break;
     const int4 tk = B.tasks[ti];
     const PanelInst& I = B.inst[tk.x];
     const int kind = tk.y, p = tk.z, r = tk.w >> 16, q = tk.w & 0xffff;
-    const int nq = I.nq;
+    const int nq = I.nq, ld = I.b;
+    TRACE_T0();
     if (tid == 0) {
       bool ok;
-      if (kind == TASK_POTRF) {
-        ok = wait_ge(&I.upd[q * nq + q], q, B.abort_flag);
-      } else if (kind == TASK_TRSM) {
+      if (kind == TASK_TRSM) {
         ok = wait_ge(&I.flag[q * nq + q], 1, B.abort_flag) && wait_ge(&I.upd[p * nq + q], q, B.abort_flag);
       } else {
         ok = wait_ge(&I.flag[p * nq + q], 1, B.abort_flag) && wait_ge(&I.flag[r * nq + q], 1, B.abort_flag) &&
@@ -85,37 +233,18 @@ __global__ void __launch_bounds__(THREADS) panel_kernel(const __grid_constant__ 
     }
     __syncthreads();
     if (!s_ok) continue;
+    TRACE_T1();
 
-    if (kind == TASK_POTRF) {
-      TileRef d = tile_of(I, q, q);
-      load<SC>(buf0, d.ptr, I.b, d.cols, d.cols, tid);
+    double acc[2][4][4];
+    zero_acc(acc);
+    if (kind == TASK_TRSM) {
+      const TileRef x = tile_of(I, p, q);
+      load_async<SG>(bufA, x.ptr, ld, x.rows, x.cols, tid);
+      load_async<SG>(bufL, I.Linv + (size_t)q * T * T, T, T, T, tid);
+      cp_async_commit();
+      cp_async_wait<0>();
       __syncthreads();
-      potrf(buf0, pairs, dg, d.cols, I.info, I.pivot_base + (long long)q * T, tid);
-      trinv(buf0, buf1, tid);
-      double* linv = I.Linv + (size_t)q * T * T;
-      for (int idx = tid; idx < T * T; idx += THREADS) {
-        const int i = idx >> 6, k = idx & 63;
-        const bool in = i < d.cols && k < d.cols;
-        if (in) d.ptr[(size_t)i * I.b + k] = buf0[i * SC + k];
-        linv[idx] = in ? buf1[i * SC + k] : 0.0;
-      }
-      // strictly-upper tiles of this tile column become zero, as in a
-      // LAPACK-style lower factor
-      for (int qq = 0; qq < q; ++qq) {
-        double* up = I.D + (size_t)(qq * T) * I.b + q * T;
-        for (int idx = tid; idx < T * T; idx += THREADS) {
-          const int i = idx >> 6, k = idx & 63;
-          if (k < d.cols) up[(size_t)i * I.b + k] = 0.0;
-        }
-      }
-    } else if (kind == TASK_TRSM) {
-      TileRef x = tile_of(I, p, q);
-      load<SG>(buf0, x.ptr, I.b, x.rows, x.cols, tid);
-      load<SG>(buf1, I.Linv + (size_t)q * T * T, T, T, T, tid);
-      __syncthreads();
-      double acc[2][4][4];
-      zero_acc(acc);
-      mma_nt(buf0, buf1, (x.cols + 3) & ~3, acc, wm, wn, g, t);
+      mma_nt(bufA, bufL, (x.cols + 3) & ~3, acc, wm, wn, g, t);
 #pragma unroll
       for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -127,19 +256,36 @@ __global__ void __launch_bounds__(THREADS) panel_kernel(const __grid_constant__ 
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
               const int col = wn * 32 + ni * 8 + 2 * t + e;
-              if (col < x.cols) x.ptr[(size_t)row * I.b + col] = acc[mi][ni][h * 2 + e];
+              if (col < x.cols) x.ptr[(size_t)row * ld + col] = acc[mi][ni][h * 2 + e];
             }
         }
+      release(&I.flag[p * nq + q], 1);
+      TRACE(kind, p, q);
     } else {
-      TileRef xp = tile_of(I, p, q);
-      TileRef xr = tile_of(I, r, q);
-      TileRef c = tile_of(I, p, r);
-      load<SG>(buf0, xp.ptr, I.b, xp.rows, xp.cols, tid);
-      load<SG>(buf1, xr.ptr, I.b, xr.rows, xr.cols, tid);
+      const TileRef xp = tile_of(I, p, q);
+      const TileRef xr = tile_of(I, r, q);
+      const TileRef c = tile_of(I, p, r);
+      load_async<SG>(bufA, xp.ptr, ld, xp.rows, xp.cols, tid);
+      load_async<SG>(bufL, xr.ptr, ld, xr.rows, xr.cols, tid);
+      cp_async_commit();
+      // prefetch the destination fragments while the operands land
+      double cv[2][2][4][2];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int row = wm * 32 + mi * 16 + g + h * 8;
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int col = wn * 32 + ni * 8 + 2 * t + e;
+              cv[mi][h][ni][e] = (row < c.rows && col < c.cols) ? __ldcg(c.ptr + (size_t)row * ld + col) : 0.0;
+            }
+        }
+      cp_async_wait<0>();
       __syncthreads();
-      double acc[2][4][4];
-      zero_acc(acc);
-      mma_nt(buf0, buf1, (xp.cols + 3) & ~3, acc, wm, wn, g, t);
+      mma_nt(bufA, bufL, (xp.cols + 3) & ~3, acc, wm, wn, g, t);
 #pragma unroll
       for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -151,23 +297,24 @@ __global__ void __launch_bounds__(THREADS) panel_kernel(const __grid_constant__ 
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
               const int col = wn * 32 + ni * 8 + 2 * t + e;
-              if (col < c.cols) {
-                double* dst = c.ptr + (size_t)row * I.b + col;
-                *dst = __ldcg(dst) - acc[mi][ni][h * 2 + e];
-              }
+              if (col < c.cols) c.ptr[(size_t)row * ld + col] = cv[mi][h][ni][e] - acc[mi][ni][h * 2 + e];
             }
         }
-    }
-    __syncthreads();
-    if (tid == 0) {
-      __threadfence();
-      if (kind == TASK_UPDATE) st_release(&I.upd[p * nq + r], q + 1);
-      else st_release(&I.flag[p * nq + q], 1);
+      release(&I.upd[p * nq + r], q + 1);
+      TRACE(kind, p, (r << 8) | q);
     }
   }
 }
 
 }  // namespace
+
+#ifdef BTA_TRACE
+extern "C" int bta_trace_setup(unsigned long long* buf) {
+  int zero = 0;
+  cudaMemcpyToSymbol(g_trace, &buf, sizeof(buf));
+  return (int)cudaMemcpyToSymbol(g_trace_n, &zero, sizeof(int));
+}
+#endif
 
 void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks) {
   int max_nq = 0;
@@ -176,11 +323,14 @@ void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks) 
     for (int ii = 0; ii < (int)insts.size(); ++ii) {
       const PanelInst& I = insts[ii];
       if (r >= I.nq) continue;
-      // updates of tile column r from every earlier column k
+      // updates of tile column r from every earlier column k (the chain CTA
+      // applies the last one to the diagonal tile itself)
       for (int k = 0; k < r; ++k)
-        for (int p = r; p < I.nrows_t; ++p) tasks.push_back(make_int4(ii, TASK_UPDATE, p, (r << 16) | k));
-      tasks.push_back(make_int4(ii, TASK_POTRF, r, (r << 16) | r));
-      for (int p = r + 1; p < I.nrows_t; ++p) tasks.push_back(make_int4(ii, TASK_TRSM, p, (r << 16) | r));
+        for (int p = r; p < I.nrows_t; ++p)
+          if (!(p == r && k == r - 1)) tasks.push_back(make_int4(ii, TASK_UPDATE, p, (r << 16) | k));
+      // TRSM below the diagonal, except the sub-diagonal tile the chain takes
+      for (int p = r + 1; p < I.nrows_t; ++p)
+        if (!(p == r + 1 && r + 1 < I.nq)) tasks.push_back(make_int4(ii, TASK_TRSM, p, (r << 16) | r));
     }
   }
 }
@@ -195,7 +345,7 @@ int panel_grid_size() {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel, THREADS, SMEM_BYTES);
-    grid = std::max(1, sms * std::max(1, occ));
+    grid = std::max(2, sms * std::max(1, occ));
   }
   return grid;
 }
@@ -204,8 +354,8 @@ int panel_launch(const PanelBatch& batch, int grid, cudaStream_t stream) {
   int g = panel_grid_size();
   if (g <= 0) return -g;
   if (grid <= 0 || grid > g) grid = g;
-  grid = std::min(grid, batch.ntasks);
-  if (grid <= 0) return cudaSuccess;
+  grid = std::min(grid, batch.ntasks + batch.ninst);
+  grid = std::max(grid, batch.ninst + (batch.ntasks > 0 ? 1 : 0));
   panel_kernel<<<grid, THREADS, SMEM_BYTES, stream>>>(batch);
   return cudaGetLastError();
 }

@@ -2,13 +2,16 @@
 //
 // The panel of step i is the tall matrix [D_i; L_i; Ab_i] (tile rows of the
 // diagonal block, of the block below it, and of the arrow), cut into 64x64
-// tiles with nq = ceil(b/64) tile columns.  The kernel factors it in place with
-// three task kinds, claimed in a fixed topological order by persistent CTAs:
+// tiles with nq = ceil(b/64) tile columns.  It is factored in place by
 //   POTRF(q)       D_i[q][q] <- chol(D_i[q][q]);  Linv_q <- its inverse
 //   TRSM(p, q)     tile(p, q) <- tile(p, q) * Linv_q^T           (p below q)
 //   UPDATE(p,r,q)  tile(p, r) <- tile(p, r) - tile(p, q) tile(r, q)^T
-// Dependencies are tracked per tile with release/acquire counters; every wait
-// is bounded and sets an abort flag instead of hanging.
+// The critical path -- TRSM(q, q-1), UPDATE(q, q, q-1), POTRF(q) for
+// q = 0..nq-1 -- runs in one dedicated "chain" CTA per instance that keeps the
+// inverse of the previous diagonal tile in shared memory.  Every other task is
+// claimed from a queue in a fixed topological order by the remaining
+// persistent CTAs.  Dependencies are tracked per tile with release/acquire
+// counters; every wait is bounded and sets an abort flag instead of hanging.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -34,8 +37,8 @@ constexpr int PANEL_MAXI = 64;
 struct PanelBatch {
   int ninst;
   int ntasks;
-  const int4* tasks;  // {inst, kind, p, (r << 16) | q}
-  int* counter;       // next task to claim
+  const int4* tasks;  // queue tasks {inst, kind, p, (r << 16) | q}
+  int* counter;       // [0] next queue task, [1] next chain role
   int* abort_flag;    // set on a timed-out wait (all later waits return)
   PanelInst inst[PANEL_MAXI];
 };
@@ -48,11 +51,11 @@ inline int panel_rows(int b, int a, bool has_L) {
   return nq + (has_L ? nq : 0) + (a + 63) / 64;
 }
 
-// Append the tasks of one instance, stage by stage, interleaving instances.
+// Queue tasks (everything except the chain) of all instances, stage by stage.
 void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks);
 
-// Launch one panel batch.  'ws_ints' must hold the counters of all instances
-// (already zeroed by the caller together with *counter and *abort_flag).
+// Launch one panel batch.  The counters of every instance, batch.counter[0..1]
+// and the abort flag must be zero-initialised by the caller.
 int panel_launch(const PanelBatch& batch, int grid, cudaStream_t stream);
 
 int panel_grid_size();

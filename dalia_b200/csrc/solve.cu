@@ -34,36 +34,52 @@ __device__ bool wait_flag(const int* p, int* abort_flag) {
 __global__ void __launch_bounds__(THREADS) diag_tile_inverse_kernel(const double* D, int n, int b, int nq,
                                                                      double* out) {
   extern __shared__ __align__(16) double sm[];
+  __shared__ double rd[T];
   double* S = sm;
-  double* Li = sm + T * SC;
+  double* Li = sm + T * SG;
   const int tid = threadIdx.x;
   const int i = blockIdx.x / nq, p = blockIdx.x % nq;
   const int w = min(T, b - p * T);
   const double* src = D + (size_t)i * b * b + (size_t)(p * T) * b + p * T;
-  load<SC>(S, src, b, w, w, tid);
+  load<SG>(S, src, b, w, w, tid);
   __syncthreads();
-  for (int r = w + tid; r < T; r += THREADS) S[r * SC + r] = 1.0;
+  for (int r = w + tid; r < T; r += THREADS) S[r * SG + r] = 1.0;
   __syncthreads();
-  trinv(S, Li, tid);
+  trinv(S, Li, rd, tid);
   double* dst = out + (size_t)blockIdx.x * T * T;
   for (int idx = tid; idx < T * T; idx += THREADS) {
     const int r = idx >> 6, c = idx & 63;
-    dst[idx] = (r < w && c < w) ? Li[r * SC + c] : 0.0;
+    dst[idx] = (r < w && c < w) ? Li[r * SG + c] : 0.0;
   }
 }
 
-// acc[r] -= sum_c M[r][c] v[c]  (rows x cols tile, leading dimension ld)
+// acc[r] -= sum_c M[r][c] v[c]  (rows x cols tile, leading dimension ld).
+// The factor is read-only during a sweep: read-only cache path, every load of
+// a lane issued before the reductions.
 __device__ __forceinline__ void gemv_sub(const double* M, int ld, int rows, int cols, const double* v,
                                          double* acc, int tid) {
   const int lane = tid & 31, warp = tid >> 5;
-  for (int r = warp; r < rows; r += 4) {
-    const double* row = M + (size_t)r * ld;
-    double s = 0.0;
-    if (lane < cols) s += __ldcg(row + lane) * v[lane];
-    if (lane + 32 < cols) s += __ldcg(row + lane + 32) * v[lane + 32];
+  const double v0 = lane < cols ? v[lane] : 0.0;
+  const double v1 = lane + 32 < cols ? v[lane + 32] : 0.0;
+  double s[16];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0) acc[r] -= s;
+  for (int j = 0; j < 16; ++j) {
+    const int r = warp + 4 * j;
+    double x = 0.0;
+    if (r < rows) {
+      const double* row = M + (size_t)r * ld;
+      if (lane < cols) x += __ldg(row + lane) * v0;
+      if (lane + 32 < cols) x += __ldg(row + lane + 32) * v1;
+    }
+    s[j] = x;
+  }
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    double x = s[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    const int r = warp + 4 * j;
+    if (lane == 0 && r < rows) acc[r] -= x;
   }
 }
 
@@ -73,8 +89,12 @@ __device__ __forceinline__ void gemv_t_sub(const double* M, int ld, int rows, in
   const int c = tid & 63, half = tid >> 6;
   double s = 0.0;
   if (c < cols) {
-    const int r0 = half * 32, r1 = min(rows, r0 + 32);
-    for (int r = r0; r < r1; ++r) s += __ldcg(M + (size_t)r * ld + c) * v[r];
+    const int r0 = half * 32;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const int r = r0 + j;
+      if (r < rows) s += __ldg(M + (size_t)r * ld + c) * v[r];
+    }
   }
   part[tid] = s;
   __syncthreads();
@@ -251,7 +271,7 @@ __global__ void arrow_backward_kernel(const double* Tt, double* x, long long nb,
 
 int diag_tile_inverses(const double* D, int n, int b, double* out, cudaStream_t s) {
   const int nq = (b + T - 1) / T;
-  const size_t smem = size_t(2) * T * SC * sizeof(double);
+  const size_t smem = size_t(2) * T * SG * sizeof(double);
   static bool attr = false;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(diag_tile_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -1,0 +1,455 @@
+"""Spatio-temporal INLA model evaluated on the GPU: theta -> BTA precision
+matrices -> f(theta) and its gradient.
+
+Host mirror of the reference's model classes for this path:
+
+* ``SpatioTemporalSubModel.construct_Q_prior`` and ``_interpretable2compute``
+  (``src/dalia/submodels/spatio_temporal.py:114-197``), plane manifold;
+* ``RegressionSubModel`` (``src/dalia/submodels/regression.py:27-35``);
+* ``Model.construct_Q_prior / construct_Q_conditional /
+  construct_information_vector`` (``src/dalia/core/model.py:306-449``);
+* ``GaussianLikelihood`` / ``PoissonLikelihood``
+  (``src/dalia/likelihoods/gaussian.py:19-131``, ``poisson.py:31-63``);
+* penalised-complexity priors
+  (``src/dalia/prior_hyperparameters/penalized_complexity.py:28-82``);
+* ``DALIA._evaluate_f`` and ``_objective_function``
+  (``src/dalia/core/dalia.py:513-745``), Serinv solver semantics (the prior
+  log-determinant comes from the BT factorisation of the spatio-temporal block,
+  so the fixed-effect tip is excluded, ``structured_solver.py:151-166``).
+
+Everything per theta runs on the device through the C ABI
+(``include/dalia_bta.h``, ``include/dalia_assemble.h``); the host only forms
+O(nt) scalar coefficients and reads back a few scalars.  Derivatives of the
+scalar coefficients use the complex-step method (all coefficient functions
+are complex-analytic), so they carry no truncation error.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+import scipy.sparse as sps
+import scipy.special as ssp
+
+from . import _lib
+
+# alpha_s = 2, alpha_t = 1, alpha_e = 1 (spatio_temporal.py:157-166)
+_ALPHA_S, _ALPHA_T, _ALPHA_E = 2, 1, 1
+_ALPHA = _ALPHA_E + _ALPHA_S * (_ALPHA_T - 0.5)
+_NU_S = _ALPHA - 1
+_NU_T = _ALPHA_T - 0.5
+_LOG_C1 = math.log(
+    ssp.gamma(_NU_T) * ssp.gamma(_NU_S)
+    / (ssp.gamma(_ALPHA_T) * ssp.gamma(_ALPHA) * pow(4 * math.pi, 1.5)))
+
+DEFAULT_PRIORS = {
+    "r_s": (0.01, 0.5),
+    "r_t": (0.01, 5.0),
+    "sigma_st": (0.01, 3.0),
+    "prec_o": (0.01, 4.0),
+}
+
+_CSTEP = 1e-30  # complex-step size
+
+
+def theta_to_gamma(r_s, r_t, sigma_st):
+    """(r_s, r_t, sigma_st) -> (gamma_s, gamma_t, gamma_st), plane manifold
+    (``spatio_temporal.py:168-193``); complex-safe."""
+    g_s = 0.5 * math.log(8 * _NU_S) - r_s
+    g_t = r_t - 0.5 * math.log(8 * _NU_T) + _ALPHA_S * g_s
+    g_st = 0.5 * _LOG_C1 - 0.5 * g_t - _NU_S * g_s - sigma_st
+    return g_s, g_t, g_st
+
+
+def pc_log_prior(kind, theta, alpha, u):
+    """Penalised-complexity log-priors (``penalized_complexity.py:55-82``);
+    complex-safe."""
+    if kind == "r_s":
+        lam = -math.log(alpha) * u  # spatial dimension 2: u^(d/2) = u
+        return math.log(lam) - lam * np.exp(-theta) - theta
+    if kind == "r_t":
+        lam = -math.log(alpha) * math.sqrt(u)
+        return math.log(lam) - lam * np.exp(-0.5 * theta) + math.log(0.5) - 0.5 * theta
+    if kind in ("sigma_st", "sigma_e", "prec_o"):
+        lam = -math.log(alpha) / u
+        return math.log(lam) - lam * np.exp(theta) + theta
+    raise ValueError(kind)
+
+
+def _tridiag(m, nt):
+    m = sps.csr_matrix(m).toarray()
+    if m.shape != (nt, nt) or np.any(np.triu(m, 2)) or np.any(np.tril(m, -2)):
+        raise ValueError("temporal FEM matrices must be tridiagonal (nt x nt)")
+    return np.diagonal(m).copy(), np.diagonal(m, -1).copy()
+
+
+def _pairs_per_row(A):
+    """All (first, second) nnz position pairs that share a row of CSR A."""
+    counts = np.diff(A.indptr)
+    row_of_p = np.repeat(np.arange(A.shape[0]), counts)
+    k_p = counts[row_of_p]
+    first = np.repeat(np.arange(A.nnz), k_p)
+    start = np.repeat(np.cumsum(k_p) - k_p, k_p)
+    j = np.arange(first.size) - start
+    second = A.indptr[row_of_p[first]] + j
+    return first, second, row_of_p
+
+
+class BTAMatrix:
+    """One BTA matrix in a single device allocation with D, L, Ab, T views."""
+
+    def __init__(self, n, b, a, device):
+        import torch
+
+        self.n, self.b, self.a = n, b, a
+        nD, nL, nA, nT = n * b * b, max(n - 1, 0) * b * b, n * a * b, a * a
+        self.offL, self.offA, self.offT = nD, nD + nL, nD + nL + nA
+        self.buf = torch.zeros(nD + nL + nA + nT, dtype=torch.float64, device=device)
+        self.D = self.buf[:nD].view(n, b, b)
+        self.L = self.buf[nD:nD + nL].view(max(n - 1, 0), b, b)
+        self.Ab = self.buf[nD + nL:nD + nL + nA].view(n, a, b)
+        self.T = self.buf[nD + nL + nA:].view(a, a)
+
+    def ptrs(self):
+        P = _lib.ptr
+        L = self.L if self.n > 1 else None
+        if self.a > 0:
+            return P(self.D), P(L), P(self.Ab), P(self.T)
+        return P(self.D), P(L), P(None), P(None)
+
+
+class SpatioTemporalModel:
+    """DEMF(1,2,1) spatio-temporal field + fixed effects, Gaussian or Poisson
+    likelihood, evaluated on one GPU."""
+
+    def __init__(self, prob, priors=None, fe_prec=1e-3, eps_gradient_f=1e-3, eps_inner_iteration=1e-3,
+                 inner_iteration_max_iter=50, device=None):
+        import torch
+
+        self.h = _lib.handle(device)
+        self.device = self.h.device
+        self.lib = _lib.load()
+        dev = self.device
+        self.ns, self.nt, self.nb = int(prob.ns), int(prob.nt), int(prob.nb)
+        n, b, a = self.nt, self.ns, self.nb
+        self.N = n * b + a
+        self.gaussian = prob.likelihood == "gaussian"
+        self.priors = dict(DEFAULT_PRIORS if priors is None else priors)
+        self.theta_keys = ["r_s", "r_t", "sigma_st"] + (["prec_o"] if self.gaussian else [])
+        self.fe_prec = float(fe_prec)
+        self.eps = float(eps_gradient_f)
+        self.eps_inner = float(eps_inner_iteration)
+        self.max_inner = int(inner_iteration_max_iter)
+
+        # --- union pattern of c0, g1, g2, g3 with four values per entry
+        U = (abs(prob.c0) + abs(prob.g1) + abs(prob.g2) + abs(prob.g3)).tocsr()
+        U.sort_indices()
+        rows = np.repeat(np.arange(b), np.diff(U.indptr))
+        cols = U.indices
+        vals4 = np.stack([np.asarray(sps.csr_matrix(K)[rows, cols]).ravel()
+                          for K in (prob.c0, prob.g1, prob.g2, prob.g3)], axis=1)
+        i32 = dict(dtype=torch.int32, device=dev)
+        f64 = dict(dtype=torch.float64, device=dev)
+        i64 = dict(dtype=torch.int64, device=dev)
+        self.u_rowptr = torch.tensor(U.indptr, **i32)
+        self.u_col = torch.tensor(cols, **i32)
+        self.u_vals4 = torch.tensor(np.ascontiguousarray(vals4), **f64)
+        self.m_diag = [_tridiag(m, n)[0] for m in (prob.m0, prob.m1, prob.m2)]
+        self.m_sub = [_tridiag(m, n)[1] for m in (prob.m0, prob.m1, prob.m2)]
+
+        # --- design matrix, responses
+        A = prob.a.tocsr()
+        A.sort_indices()
+        self.A_host = A
+        self.nobs = A.shape[0]
+        self.y_host = np.asarray(prob.y, dtype=np.float64)
+        self.e_host = np.ones(self.nobs) if prob.e is None else np.asarray(prob.e, dtype=np.float64)
+        self.A_rowptr = torch.tensor(A.indptr.astype(np.int64), **i64)
+        self.A_col = torch.tensor(A.indices.astype(np.int32), **i32)
+        self.A_val = torch.tensor(A.data, **f64)
+        AT = A.T.tocsr()
+        AT.sort_indices()
+        self.AT_rowptr = torch.tensor(AT.indptr.astype(np.int64), **i64)
+        self.AT_col = torch.tensor(AT.indices.astype(np.int32), **i32)
+        self.AT_val = torch.tensor(AT.data, **f64)
+        self.y = torch.tensor(self.y_host, **f64)
+        self.e = torch.tensor(self.e_host, **f64)
+        X = A[:, n * b:].toarray() if a > 0 else np.zeros((self.nobs, 0))
+        self.X = torch.tensor(np.ascontiguousarray(X), **f64)
+        self.XtX_host = X.T @ X
+        self.yty = float(self.y_host @ self.y_host)
+        self.Aty = torch.tensor(A.T @ self.y_host, **f64)
+
+        # --- A^T D A entry lists on the BTA pattern (tip handled separately)
+        self.Qc = BTAMatrix(n, b, a, dev)
+        self.Qp = BTAMatrix(n, b, 0, dev)
+        first, second, row_of_p = _pairs_per_row(A)
+        c1, c2 = A.indices[first], A.indices[second]
+        fac = A.data[first] * A.data[second]
+        obs = row_of_p[first]
+        nbt = n * b
+        bi, bj = c1 // b, c2 // b
+        inD = (c1 < nbt) & (c2 < nbt) & (bi == bj)
+        inL = (c1 < nbt) & (c2 < nbt) & (bi == bj + 1)
+        inA = (c1 >= nbt) & (c2 < nbt)
+        bad = (c1 < nbt) & (c2 < nbt) & (np.abs(bi - bj) > 1)
+        if np.any(bad):
+            raise ValueError("design matrix couples latent blocks more than one time step apart")
+        dst = np.full(c1.shape, -1, dtype=np.int64)
+        dst[inD] = (bi[inD] * b + c1[inD] % b) * b + c2[inD] % b
+        dst[inL] = self.Qc.offL + (bj[inL] * b + c1[inL] % b) * b + c2[inL] % b
+        dst[inA] = self.Qc.offA + ((c2[inA] // b) * a + (c1[inA] - nbt)) * b + c2[inA] % b
+        keep = dst >= 0
+        dst, obs, fac = dst[keep], obs[keep], fac[keep]
+        kindmult = np.where(inD[keep], 1.0, 2.0)
+        order = np.argsort(dst, kind="stable")
+        dst, obs, fac, kindmult = dst[order], obs[order], fac[order], kindmult[order]
+        ud, start = np.unique(dst, return_index=True)
+        off = np.append(start, dst.size).astype(np.int64)
+        self.ent_dst = torch.tensor(ud, **i64)
+        self.ent_off = torch.tensor(off, **i64)
+        self.ent_obs = torch.tensor(obs.astype(np.int32), **i32)
+        self.ent_fac = torch.tensor(fac, **f64)
+        self.nent = int(ud.size)
+        # trace weights of A^T A on the stored entries (lower blocks count twice)
+        sumfac = np.add.reduceat(fac, start) if fac.size else np.zeros(0)
+        self.ata_w = torch.tensor(sumfac * kindmult[start], **f64)
+
+        # --- scratch
+        self.nparts = 148
+        self.part = torch.zeros(4096, **f64)
+        self.scal = torch.zeros(64, **f64)
+        self.coef_dev = torch.zeros((2 * n - 1) * 4, **f64)
+        self.coef_host = torch.zeros((2 * n - 1) * 4, dtype=torch.float64).pin_memory()
+        self.rhs = torch.zeros(self.N, **f64)
+        self.x = torch.zeros(self.N, **f64)  # latent mode / mean, like model.x
+        self.eta = torch.zeros(self.nobs, **f64)
+        self.dvec = torch.zeros(self.nobs, **f64)
+        self.inner_c = torch.zeros((2 * n - 1) * 4, **f64)
+        self.inner_p = torch.zeros((2 * n - 1) * 4, **f64)
+        self.quad_st = torch.zeros((2 * n - 1) * 4, **f64)
+
+    # ------------------------------------------------------------------ host
+    def coef_blocks(self, theta):
+        """Coefficients of (c0, g1, g2, g3) for every lower BTA block of Q_st;
+        rows 0..n-1 diagonal blocks, rows n..2n-2 sub-diagonal blocks.
+        Complex-safe."""
+        g_s, g_t, g_st = theta_to_gamma(theta[0], theta[1], theta[2])
+        k2 = np.exp(2 * g_s)
+        E = np.exp(2 * g_st)
+        u = np.exp(g_t)
+        m0 = np.concatenate([self.m_diag[0], self.m_sub[0]])
+        m1 = np.concatenate([self.m_diag[1], self.m_sub[1]])
+        m2 = np.concatenate([self.m_diag[2], self.m_sub[2]])
+        # q1 = k2 c0 + g1; q2 = k2^2 c0 + 2 k2 g1 + g2; q3 = k2^3 c0 + 3 k2^2 g1 + 3 k2 g2 + g3
+        c_c0 = E * (m0 * k2 ** 3 + u * m1 * k2 ** 2 + u * u * m2 * k2)
+        c_g1 = E * (3 * m0 * k2 ** 2 + 2 * u * m1 * k2 + u * u * m2)
+        c_g2 = E * (3 * m0 * k2 + u * m1)
+        c_g3 = E * m0
+        return np.stack([c_c0, c_g1, c_g2, c_g3], axis=1)
+
+    def log_prior_theta(self, theta):
+        s = 0.0
+        for k, key in enumerate(self.theta_keys):
+            al, u = self.priors[key]
+            s = s + pc_log_prior(key, theta[k], al, u)
+        return s
+
+    def lik0(self, theta):
+        """Gaussian log-likelihood at eta = 0 (``gaussian.py:55-62``)."""
+        return 0.5 * theta[-1] * self.nobs - 0.5 * np.exp(theta[-1]) * self.yty
+
+    # ---------------------------------------------------------------- device
+    def _stream(self):
+        return _lib.stream_ptr(self.device)
+
+    def _check(self, rc, what):
+        _lib.check(rc, what)
+
+    def _assemble_prior(self, theta, M: BTAMatrix):
+        c = np.asarray(self.coef_blocks(theta), dtype=np.float64).ravel()
+        self.coef_host.numpy()[:] = c
+        self.coef_dev.copy_(self.coef_host, non_blocking=True)
+        D, L, _, _ = M.ptrs()
+        self._check(self.lib.bta_assemble_prior(self._stream(), M.n, M.b, _lib.ptr(self.coef_dev),
+                                                _lib.ptr(self.u_rowptr), _lib.ptr(self.u_col),
+                                                _lib.ptr(self.u_vals4), D, L), "assemble_prior")
+
+    def assemble_conditional(self, theta, d=None, dscale=1.0):
+        """Q_c = Q_prior + A^T diag(dscale * d) A in BTA storage (``model.py:384-423``);
+        d None means the Gaussian constant diagonal."""
+        Q = self.Qc
+        self._assemble_prior(theta, Q)
+        if Q.a > 0:
+            Q.Ab.zero_()
+        dptr = _lib.ptr(d)
+        self._check(self.lib.bta_add_entries(self._stream(), self.nent, _lib.ptr(self.ent_dst),
+                                             _lib.ptr(self.ent_off), _lib.ptr(self.ent_obs), _lib.ptr(self.ent_fac),
+                                             dptr, float(dscale), _lib.ptr(Q.buf)), "add_entries")
+        if Q.a > 0:
+            self._check(self.lib.bta_arrow_tip(self._stream(), self.nobs, Q.a, _lib.ptr(self.X), dptr,
+                                               self.fe_prec, float(dscale), _lib.ptr(self.part), self.nparts,
+                                               _lib.ptr(Q.T)), "arrow_tip")
+
+    def assemble_prior_bt(self, theta):
+        self._assemble_prior(theta, self.Qp)
+
+    def factor(self, M: BTAMatrix):
+        D, L, Ab, T = M.ptrs()
+        self._check(self.lib.bta_pobtaf(self.h.bind_stream(), M.n, M.b, M.a, D, L, Ab, T, None), "pobtaf")
+
+    def logdet_to(self, M: BTAMatrix, slot):
+        D, _, _, T = M.ptrs()
+        out = _lib.ptr(self.scal[slot:slot + 1])
+        self._check(self.lib.bta_logdet(self.h.bind_stream(), M.n, M.b, M.a, D, T, 1 if M.a else 0, out, None),
+                    "logdet")
+
+    def sweep(self, M: BTAMatrix, x, trans):
+        D, L, Ab, T = M.ptrs()
+        self._check(self.lib.bta_pobtas(self.h.bind_stream(), M.n, M.b, M.a, D, L, Ab, T, _lib.ptr(x), trans),
+                    "pobtas")
+
+    def selinv(self, M: BTAMatrix):
+        D, L, Ab, T = M.ptrs()
+        self._check(self.lib.bta_pobtasi(self.h.bind_stream(), M.n, M.b, M.a, D, L, Ab, T), "pobtasi")
+
+    def dot_to(self, x, y, slot):
+        self._check(self.lib.bta_dot(self._stream(), x.numel(), _lib.ptr(x), _lib.ptr(y), _lib.ptr(self.part),
+                                     self.nparts, _lib.ptr(self.scal[slot:slot + 1])), "dot")
+
+    def spmv(self, rowptr, col, val, m, x, y, alpha=1.0, beta=0.0):
+        self._check(self.lib.bta_csr_spmv(self._stream(), m, _lib.ptr(rowptr), _lib.ptr(col), _lib.ptr(val),
+                                          _lib.ptr(x), float(alpha), float(beta), _lib.ptr(y)), "spmv")
+
+    def status(self):
+        info = ctypes.c_int64(0)
+        rc = self.lib.bta_get_status(self.h.bind_stream(), ctypes.byref(info))
+        if rc == _lib.BTA_ERR_NOT_SPD:
+            raise np.linalg.LinAlgError(f"precision matrix not positive definite (pivot {info.value})")
+        _lib.check(rc, "status")
+
+    # ------------------------------------------------------------ objective
+    def evaluate_f(self, theta):
+        """f(theta) following ``DALIA._evaluate_f`` (``dalia.py:603-745``)."""
+        theta = np.asarray(theta, dtype=np.float64)
+        _lib.check(self.lib.bta_reset_status(self.h.bind_stream()), "reset")
+        if self.gaussian:
+            tau = math.exp(theta[-1])
+            self.assemble_conditional(theta, None, tau)
+            self.factor(self.Qc)
+            self.logdet_to(self.Qc, 0)
+            # rhs = -Q_prior x + A^T grad(lik) at x = 0, eta = 0  ->  tau A^T y
+            self._check(self.lib.bta_axpby(self._stream(), self.N, tau, _lib.ptr(self.Aty), 0.0,
+                                           _lib.ptr(self.rhs)), "axpby")
+            self.x.copy_(self.rhs)
+            self.sweep(self.Qc, self.x, 0)
+            self.sweep(self.Qc, self.x, 1)
+            self.dot_to(self.rhs, self.x, 1)  # mu^T Q_c mu = b^T mu
+            self.assemble_prior_bt(theta)
+            self.factor(self.Qp)
+            self.logdet_to(self.Qp, 2)
+            self.status()
+            s = self.scal[:3].cpu().numpy()
+            cond = 0.5 * s[0] - 0.5 * s[1]
+            f = cond - (self.log_prior_theta(theta) + self.lik0(theta) + 0.5 * s[2])
+        else:
+            f = self._evaluate_f_poisson(theta)
+        if np.isnan(f):
+            raise ValueError("f(theta) is NaN. Check what is happening.")
+        return float(f)
+
+    def objective_fd(self, theta):
+        """(f, central finite-difference gradient): the reference's
+        ``_objective_function`` (``dalia.py:513-601``), evaluated point by point
+        in reverse order."""
+        theta = np.asarray(theta, dtype=np.float64)
+        d = theta.size
+        nf = 2 * d + 1
+        tm = np.repeat(theta.reshape(-1, 1), nf, axis=1)
+        tm[:, 1:1 + d] += self.eps * np.eye(d)
+        tm[:, d + 1:nf] -= self.eps * np.eye(d)
+        fv = np.zeros(nf)
+        for k in range(nf - 1, -1, -1):
+            fv[k] = self.evaluate_f(tm[:, k])
+        return fv[0], (fv[1:1 + d] - fv[d + 1:nf]) / (2 * self.eps)
+
+    def _dcoef(self, theta, k):
+        th = np.asarray(theta, dtype=np.complex128).copy()
+        th[k] += 1j * _CSTEP
+        return np.imag(self.coef_blocks(th)) / _CSTEP
+
+    def _dfun(self, fun, theta, k):
+        th = np.asarray(theta, dtype=np.complex128).copy()
+        th[k] += 1j * _CSTEP
+        return float(np.imag(fun(th)) / _CSTEP)
+
+    def objective_adjoint(self, theta):
+        """(f, exact gradient) from one factorisation + selected inversion of
+        Q_c and of Q_prior:
+        df/dth = 1/2 tr(S_c dQ_c) - 1/2 tr(S_p dQ_st) + 1/2 mu^T dQ_c mu
+                 - mu^T db - d log p(theta) - d lik0,
+        with tr(S dQ_st) and mu^T dQ_st mu contracted block by block against
+        the Kronecker factors (c0, g1, g2, g3) and S = Q^{-1} on the BTA
+        pattern (Gaussian likelihood)."""
+        if not self.gaussian:
+            raise NotImplementedError("adjoint gradient: Gaussian likelihood")
+        import torch
+
+        theta = np.asarray(theta, dtype=np.float64)
+        n, b, a = self.nt, self.ns, self.nb
+        tau = math.exp(theta[-1])
+        stream = self._stream()
+        _lib.check(self.lib.bta_reset_status(self.h.bind_stream()), "reset")
+        self.assemble_conditional(theta, None, tau)
+        self.factor(self.Qc)
+        self.logdet_to(self.Qc, 0)
+        self._check(self.lib.bta_axpby(stream, self.N, tau, _lib.ptr(self.Aty), 0.0, _lib.ptr(self.rhs)), "axpby")
+        self.x.copy_(self.rhs)
+        self.sweep(self.Qc, self.x, 0)
+        self.dot_to(self.x, self.x, 1)  # b^T Q^-1 b = |L^-1 b|^2
+        self.sweep(self.Qc, self.x, 1)  # mu
+        self.assemble_prior_bt(theta)
+        self.factor(self.Qp)
+        self.logdet_to(self.Qp, 2)
+        # |A mu|^2 and mu^T (E_tt' (x) K) mu
+        self.spmv(self.A_rowptr, self.A_col, self.A_val, self.nobs, self.x, self.eta)
+        self.dot_to(self.eta, self.eta, 3)
+        self._check(self.lib.bta_block_quad(stream, n, b, _lib.ptr(self.u_rowptr), _lib.ptr(self.u_col),
+                                            _lib.ptr(self.u_vals4), _lib.ptr(self.x), _lib.ptr(self.quad_st)),
+                    "block_quad")
+        # selected inverses and their contractions
+        self.selinv(self.Qc)
+        self.selinv(self.Qp)
+        Dc, Lc, _, _ = self.Qc.ptrs()
+        Dp, Lp, _, _ = self.Qp.ptrs()
+        for (Dm, Lm, out) in ((Dc, Lc, self.inner_c), (Dp, Lp, self.inner_p)):
+            self._check(self.lib.bta_block_inner(stream, n, b, _lib.ptr(self.u_rowptr), _lib.ptr(self.u_col),
+                                                 _lib.ptr(self.u_vals4), Dm, Lm, _lib.ptr(out)), "block_inner")
+        self._check(self.lib.bta_gather_dot(stream, self.nent, _lib.ptr(self.ent_dst), _lib.ptr(self.ata_w),
+                                            _lib.ptr(self.Qc.buf), _lib.ptr(self.part), self.nparts,
+                                            _lib.ptr(self.scal[4:5])), "gather_dot")
+        self.status()
+        s = self.scal[:5].cpu().numpy()
+        Ic = self.inner_c.view(-1, 4).cpu().numpy()
+        Ip = self.inner_p.view(-1, 4).cpu().numpy()
+        Qm = self.quad_st.view(-1, 4).cpu().numpy()
+        Tsel = self.Qc.T.cpu().numpy()
+        mult = np.ones((2 * n - 1, 1))
+        mult[n:] = 2.0  # each sub-diagonal block appears twice in the symmetric matrix
+        f = 0.5 * s[0] - 0.5 * s[1] - (self.log_prior_theta(theta) + self.lik0(theta) + 0.5 * s[2])
+        grad = np.zeros(theta.size)
+        for k in range(3):
+            dc = self._dcoef(theta, k) * mult
+            grad[k] = (0.5 * np.sum(dc * Ic) - 0.5 * np.sum(dc * Ip) + 0.5 * np.sum(dc * Qm)
+                       - self._dfun(self.log_prior_theta, theta, k))
+        tr_ata = s[4] + float(np.sum(Tsel * self.XtX_host))
+        grad[-1] = (0.5 * tau * tr_ata - s[1] + 0.5 * tau * s[3]
+                    - (0.5 * self.nobs - 0.5 * tau * self.yty)
+                    - self._dfun(self.log_prior_theta, theta, theta.size - 1))
+        return float(f), grad
+
+    # ------------------------------------------------------------- Poisson
+    def _evaluate_f_poisson(self, theta):
+        raise NotImplementedError("Poisson likelihood on the device path")

@@ -48,9 +48,11 @@ size_t bta_workspace_bytes(bta_handle_t handle);
  * called at src/dalia/solvers/structured_solver.py:83-88.
  * On exit D holds the lower factors (zeros above the diagonal), L, Ab and T the
  * factor blocks.  a = 0 gives the BT factorisation (pobtf, :90-93); Ab and T
- * may then be NULL.  If info != NULL the call synchronises the stream and
- * writes 0 on success or the 1-based global index of the first non-positive
- * pivot (then returns BTA_ERR_NOT_SPD).
+ * may then be NULL.  If info != NULL the call clears the handle's status,
+ * synchronises the stream and writes 0 on success or the 1-based global index
+ * of the first non-positive pivot (then returns BTA_ERR_NOT_SPD).  With
+ * info == NULL the call is asynchronous and the status accumulates on the
+ * handle until bta_get_status / bta_reset_status.
  */
 int bta_pobtaf(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, double* L, double* Ab, double* T,
                int64_t* info);
@@ -86,6 +88,9 @@ int bta_logdet(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D,
  * BTA_ERR_NOT_SPD / BTA_ERR_TIMEOUT accordingly.
  */
 int bta_get_status(bta_handle_t h, int64_t* info);
+
+/* Clear the handle's status (stream-ordered). */
+int bta_reset_status(bta_handle_t h);
 
 /*
  * Scatter a COO matrix (row, col, val; nnz entries, symmetric storage as

@@ -233,3 +233,70 @@ class OracleModel:
         bta_ref.pobtasi(D, L, Ab, T)
         return np.concatenate([np.concatenate([np.diagonal(D[i]) for i in range(self.nt)]),
                                np.diagonal(T)])
+
+
+# ---------------------------------------------------------------------------
+# Dense adjoint gradient (test oracle for the GPU adjoint).  For a Gaussian
+# likelihood, with S_c = Q_c^{-1}, S_p = Q_st^{-1}, mu = Q_c^{-1} b:
+#   df/dth_k = 1/2 tr(S_c dQ_c) - 1/2 tr(S_p dQ_st) + 1/2 mu^T dQ_c mu - mu^T db
+#              - d log p(theta) - d lik(eta=0),
+# with dQ obtained by the complex-step method on the restated assembly.
+
+def _cstep(fun, theta, k, h=1e-30):
+    th = np.asarray(theta, dtype=np.complex128).copy()
+    th[k] += 1j * h
+    return np.imag(fun(th)) / h
+
+
+def _q_st_complex(model, theta):
+    p = model.p
+    g_s = 0.5 * math.log(8 * _NU_S) - theta[0]
+    g_t = theta[1] - 0.5 * math.log(8 * _NU_T) + _ALPHA_S * g_s
+    g_st = 0.5 * math.log(_C1) - 0.5 * g_t - _NU_S * g_s - theta[2]
+    es, et, est = np.exp(g_s), np.exp(g_t), np.exp(g_st)
+    q1 = es ** 2 * p.c0 + p.g1
+    q2 = es ** 4 * p.c0 + 2 * es ** 2 * p.g1 + p.g2
+    q3 = es ** 6 * p.c0 + 3 * es ** 4 * p.g1 + 3 * es ** 2 * p.g2 + p.g3
+    return (est ** 2 * (sps.kron(p.m0, q3) + et * sps.kron(p.m1, q2) + et ** 2 * sps.kron(p.m2, q1))).toarray()
+
+
+def _log_prior_complex(model, theta):
+    s = 0.0
+    for k, key in enumerate(model.theta_keys):
+        al, u = model.priors[key]
+        if key == "r_s":
+            lam = -math.log(al) * u
+            s = s + math.log(lam) - lam * np.exp(-theta[k]) - theta[k]
+        elif key == "r_t":
+            lam = -math.log(al) * math.sqrt(u)
+            s = s + math.log(lam) - lam * np.exp(-0.5 * theta[k]) + math.log(0.5) - 0.5 * theta[k]
+        else:
+            lam = -math.log(al) / u
+            s = s + math.log(lam) - lam * np.exp(theta[k]) + theta[k]
+    return s
+
+
+def dense_adjoint_gradient(model: OracleModel, theta):
+    theta = np.asarray(theta, dtype=np.float64)
+    assert model.gaussian
+    nst = model.ns * model.nt
+    tau = math.exp(theta[-1])
+    Qc = model.q_cond(theta, np.zeros(len(model.y))).toarray()
+    Qst = model.q_st(theta).toarray()
+    Sc = np.linalg.inv(Qc)
+    Sp = np.linalg.inv(Qst)
+    Ad = model.A.toarray()
+    b = tau * (Ad.T @ model.y)
+    mu = Sc @ b
+    grad = np.zeros(theta.size)
+    for k in range(3):
+        dQ = _cstep(lambda th: _q_st_complex(model, th), theta, k)
+        dQc = np.zeros_like(Qc)
+        dQc[:nst, :nst] = dQ
+        grad[k] = (0.5 * np.sum(Sc * dQc) - 0.5 * np.sum(Sp * dQ) + 0.5 * mu @ dQc @ mu
+                   - _cstep(lambda th: _log_prior_complex(model, th), theta, k))
+    dQc = tau * (Ad.T @ Ad)
+    dlik = 0.5 * len(model.y) - 0.5 * tau * (model.y @ model.y)
+    grad[-1] = (0.5 * np.sum(Sc * dQc) + 0.5 * mu @ dQc @ mu - mu @ b - dlik
+                - _cstep(lambda th: _log_prior_complex(model, th), theta, theta.size - 1))
+    return grad

@@ -79,3 +79,18 @@ def test_config0_scalars_match_reference():
     f = om.evaluate_f(g["theta"])
     assert abs(f - float(g["f_serinv"])) < 1e-10 * abs(float(g["f_serinv"]))
     assert rel(om.x, g["x_dense"]) < 1e-9
+
+
+@pytest.mark.parametrize("name", GAUSS)
+def test_dense_adjoint_matches_reference_fd_gradient(name):
+    """The adjoint formula (dense oracle) agrees with the reference's own FD
+    gradient up to the FD truncation error (eps = 1e-3), and with a finer
+    oracle FD to ~1e-8."""
+    g = load(name)
+    prob = problem(g)
+    om = model_ref.OracleModel(prob)
+    ga = model_ref.dense_adjoint_gradient(om, g["theta"])
+    assert rel(ga, g["grad_serinv"]) < 1e-5
+    om.eps = 1e-5
+    _, gfd = om.objective(g["theta"])
+    assert rel(ga, gfd) < 1e-7
