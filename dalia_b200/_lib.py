@@ -41,6 +41,9 @@ SIGNATURES = {
     "bta_logdet": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _int, _c_void_p, _pdbl]),
     "bta_get_status": (_int, [_c_void_p, _pi64]),
     "bta_reset_status": (_int, [_c_void_p]),
+    "bta_launch_count": (ctypes.c_longlong, []),
+    "bta_prof_enable": (_int, [_int]),
+    "bta_prof_read": (_int, [_pdbl, ctypes.POINTER(ctypes.c_longlong)]),
     "bta_gather_coo": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _i64, _int,
                               _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p]),
     "bta_scatter_coo": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _i64, _int,

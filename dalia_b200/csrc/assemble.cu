@@ -13,6 +13,7 @@
 
 #include "../../include/dalia_assemble.h"
 #include "../../include/dalia_bta.h"
+#include "prof.cuh"
 
 namespace {
 
@@ -272,8 +273,14 @@ extern "C" {
 
 int bta_dot(void* stream, int64_t n, const double* x, const double* y, double* part, int nparts, double* out) {
   if (n < 0 || nparts < 1 || !part || !out) return BTA_ERR_INVALID;
-  dot_kernel<<<nparts, 256, 0, (cudaStream_t)stream>>>(n, x, y, part);
-  sum_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(part, nparts, out);
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    dot_kernel<<<nparts, 256, 0, (cudaStream_t)stream>>>(n, x, y, part);
+  }
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    sum_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(part, nparts, out);
+  }
   return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
 }
 
@@ -281,7 +288,10 @@ int bta_axpby(void* stream, int64_t n, double alpha, const double* x, double bet
   if (n < 0 || (n > 0 && (!x || !y))) return BTA_ERR_INVALID;
   if (n == 0) return BTA_OK;
   const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
-  axpby_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(n, alpha, x, beta, y);
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    axpby_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(n, alpha, x, beta, y);
+  }
   return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
 }
 
@@ -291,8 +301,11 @@ int bta_assemble_prior(void* stream, int64_t n, int64_t b, const double* coef, c
   if (n < 1 || b < 1 || !coef || !rowptr || !colidx || !vals4 || !D || (n > 1 && !L)) return BTA_ERR_INVALID;
   const int slabs = (int)((b + 7) / 8);
   const int nblk = (int)(2 * n - 1);
-  assemble_prior_kernel<<<nblk * slabs, 256, 0, (cudaStream_t)stream>>>((int)n, (int)b, coef, rowptr, colidx, vals4,
-                                                                       D, L);
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    assemble_prior_kernel<<<nblk * slabs, 256, 0, (cudaStream_t)stream>>>((int)n, (int)b, coef, rowptr, colidx, vals4,
+                                                                         D, L);
+  }
   return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
 }
 
@@ -301,38 +314,59 @@ int bta_add_entries(void* stream, int64_t nent, const int64_t* dst, const int64_
   if (nent < 0 || (nent > 0 && (!dst || !off || !base))) return BTA_ERR_INVALID;
   if (nent == 0) return BTA_OK;
   const int grid = (int)std::min<int64_t>((nent + 255) / 256, 148 * 16);
-  add_entries_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(nent, dst, off, obs, fac, d, dscale, base);
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    add_entries_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(nent, dst, off, obs, fac, d, dscale, base);
+  }
   return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
 }
 
 int bta_arrow_tip(void* stream, int64_t nobs, int64_t a, const double* X, const double* d, double prec,
                   double dscale, double* part, int nparts, double* T) {
   if (a < 1 || nobs < 0 || !X || !T || !part || nparts < 1) return BTA_ERR_INVALID;
-  tip_partial_kernel<<<nparts, 256, 256 * sizeof(double), (cudaStream_t)stream>>>(nobs, (int)a, X, d, part);
-  tip_final_kernel<<<1, 128, 0, (cudaStream_t)stream>>>(nparts, (int)a, part, prec, dscale, T);
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    tip_partial_kernel<<<nparts, 256, 256 * sizeof(double), (cudaStream_t)stream>>>(nobs, (int)a, X, d, part);
+  }
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    tip_final_kernel<<<1, 128, 0, (cudaStream_t)stream>>>(nparts, (int)a, part, prec, dscale, T);
+  }
   return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
 }
 
 int bta_block_inner(void* stream, int64_t n, int64_t b, const int* rowptr, const int* colidx, const double* vals4,
                     const double* D, const double* L, double* out) {
   if (n < 1 || b < 1 || !out) return BTA_ERR_INVALID;
-  block_inner_kernel<<<(int)(2 * n - 1), 256, 0, (cudaStream_t)stream>>>((int)n, (int)b, rowptr, colidx, vals4, D, L,
-                                                                       out);
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    block_inner_kernel<<<(int)(2 * n - 1), 256, 0, (cudaStream_t)stream>>>((int)n, (int)b, rowptr, colidx, vals4, D, L,
+                                                                         out);
+  }
   return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
 }
 
 int bta_block_quad(void* stream, int64_t n, int64_t b, const int* rowptr, const int* colidx, const double* vals4,
                    const double* x, double* out) {
   if (n < 1 || b < 1 || !out || !x) return BTA_ERR_INVALID;
-  block_quad_kernel<<<(int)(2 * n - 1), 256, 0, (cudaStream_t)stream>>>((int)n, (int)b, rowptr, colidx, vals4, x, out);
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    block_quad_kernel<<<(int)(2 * n - 1), 256, 0, (cudaStream_t)stream>>>((int)n, (int)b, rowptr, colidx, vals4, x, out);
+  }
   return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
 }
 
 int bta_gather_dot(void* stream, int64_t nent, const int64_t* idx, const double* w, const double* base, double* part,
                    int nparts, double* out) {
   if (nent < 0 || nparts < 1 || !part || !out) return BTA_ERR_INVALID;
-  gather_dot_kernel<<<nparts, 256, 0, (cudaStream_t)stream>>>(nent, idx, w, base, part);
-  sum_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(part, nparts, out);
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    gather_dot_kernel<<<nparts, 256, 0, (cudaStream_t)stream>>>(nent, idx, w, base, part);
+  }
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    sum_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(part, nparts, out);
+  }
   return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
 }
 
@@ -341,7 +375,10 @@ int bta_csr_spmv(void* stream, int64_t m, const int64_t* rowptr, const int* col,
   if (m < 0 || (m > 0 && (!rowptr || !x || !y))) return BTA_ERR_INVALID;
   if (m == 0) return BTA_OK;
   const int grid = (int)std::min<int64_t>((m * 32 + 255) / 256, 148 * 32);
-  csr_spmv_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(m, rowptr, col, val, x, alpha, beta, y);
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    csr_spmv_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(m, rowptr, col, val, x, alpha, beta, y);
+  }
   return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
 }
 
@@ -349,8 +386,11 @@ int bta_symv(void* stream, int64_t n, int64_t b, int64_t a, const double* D, con
              const double* T, const double* x, double* y) {
   if (n < 1 || b < 1 || a < 0 || !D || !x || !y) return BTA_ERR_INVALID;
   const int64_t rows = n * b + a;
-  bta_symv_kernel<<<(int)((rows + 7) / 8), 256, 0, (cudaStream_t)stream>>>((int)n, (int)b, (int)a, D, L, Ab, T, x,
-                                                                          y);
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    bta_symv_kernel<<<(int)((rows + 7) / 8), 256, 0, (cudaStream_t)stream>>>((int)n, (int)b, (int)a, D, L, Ab, T, x,
+                                                                            y);
+  }
   return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
 }
 

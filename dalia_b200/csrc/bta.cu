@@ -11,6 +11,7 @@
 #include "bta_internal.cuh"
 #include "gemm.cuh"
 #include "panel.cuh"
+#include "prof.cuh"
 
 using namespace bta;
 
@@ -421,7 +422,10 @@ int bta_gather_coo(bta_handle_t h, int64_t n, int64_t b, int64_t a, const int64_
   if (!sparsity_bt && a > 0 && (!Ab || !T)) return BTA_ERR_INVALID;
   if (nnz > 0) {
     const int grid = (int)std::min<int64_t>((nnz + 255) / 256, 148 * 32);
-    gather_coo_kernel<<<grid, 256, 0, h->stream>>>(row, col, nnz, n, b, a, sparsity_bt, D, L, Ab, T, out);
+    {
+      bta::ProfScope _ps(bta::PROF_OTHER, h->stream);
+      gather_coo_kernel<<<grid, 256, 0, h->stream>>>(row, col, nnz, n, b, a, sparsity_bt, D, L, Ab, T, out);
+    }
   }
   return cuda_rc(cudaGetLastError());
 }
@@ -440,7 +444,10 @@ int bta_scatter_coo(bta_handle_t h, int64_t n, int64_t b, int64_t a, const int64
   }
   if (nnz > 0) {
     const int grid = (int)std::min<int64_t>((nnz + 255) / 256, 148 * 32);
-    scatter_coo_kernel<<<grid, 256, 0, s>>>(row, col, val, nnz, n, b, a, sparsity_bt, D, L, Ab, T);
+    {
+      bta::ProfScope _ps(bta::PROF_OTHER, s);
+      scatter_coo_kernel<<<grid, 256, 0, s>>>(row, col, val, nnz, n, b, a, sparsity_bt, D, L, Ab, T);
+    }
   }
   return cuda_rc(cudaGetLastError());
 }

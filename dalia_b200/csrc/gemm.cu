@@ -7,6 +7,7 @@
 
 #include "common.cuh"
 #include "gemm.cuh"
+#include "prof.cuh"
 
 namespace bta {
 namespace {
@@ -230,7 +231,10 @@ int gemm_launch(const std::vector<GemmProb>& probs, cudaStream_t stream) {
     }
     if (b.count == 0) continue;
     b.tile_start[b.count] = total;
-    gemm_f64_kernel<<<total, THREADS, SMEM_BYTES, stream>>>(b);
+    {
+      bta::ProfScope _ps(bta::PROF_GEMM, stream);
+      gemm_f64_kernel<<<total, THREADS, SMEM_BYTES, stream>>>(b);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

@@ -4,6 +4,7 @@
 #include "common.cuh"
 #include "panel.cuh"
 #include "tile_ops.cuh"
+#include "prof.cuh"
 
 namespace bta {
 namespace {
@@ -356,7 +357,10 @@ int panel_launch(const PanelBatch& batch, int grid, cudaStream_t stream) {
   if (grid <= 0 || grid > g) grid = g;
   grid = std::min(grid, batch.ntasks + batch.ninst);
   grid = std::max(grid, batch.ninst + (batch.ntasks > 0 ? 1 : 0));
-  panel_kernel<<<grid, THREADS, SMEM_BYTES, stream>>>(batch);
+  {
+    bta::ProfScope _ps(bta::PROF_PANEL, stream);
+    panel_kernel<<<grid, THREADS, SMEM_BYTES, stream>>>(batch);
+  }
   return cudaGetLastError();
 }
 

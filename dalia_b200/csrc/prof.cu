@@ -1,0 +1,89 @@
+// Launch counter and optional per-category CUDA-event timing (prof.cuh).
+#include <atomic>
+#include <mutex>
+#include <vector>
+
+#include "../../include/dalia_bta.h"
+#include "prof.cuh"
+
+namespace bta {
+namespace {
+
+struct Pending {
+  int cat;
+  cudaEvent_t a, b;
+};
+
+std::atomic<long long> g_launches{0};
+std::atomic<bool> g_on{false};
+std::mutex g_mu;
+std::vector<Pending> g_pending;
+std::vector<cudaEvent_t> g_pool;
+double g_ms[PROF_NCAT] = {0};
+long long g_cnt[PROF_NCAT] = {0};
+
+cudaEvent_t take_event() {
+  if (!g_pool.empty()) {
+    cudaEvent_t e = g_pool.back();
+    g_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+}  // namespace
+
+void prof_begin(int cat, cudaStream_t s, cudaEvent_t* ev) {
+  (void)cat;
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  *ev = nullptr;
+  if (!g_on.load(std::memory_order_relaxed)) return;
+  std::lock_guard<std::mutex> lk(g_mu);
+  *ev = take_event();
+  cudaEventRecord(*ev, s);
+}
+
+void prof_end(int cat, cudaStream_t s, cudaEvent_t ev) {
+  if (ev == nullptr) return;
+  std::lock_guard<std::mutex> lk(g_mu);
+  cudaEvent_t e2 = take_event();
+  cudaEventRecord(e2, s);
+  g_pending.push_back({cat, ev, e2});
+}
+
+}  // namespace bta
+
+extern "C" {
+
+long long bta_launch_count(void) { return bta::g_launches.load(); }
+
+int bta_prof_enable(int on) {
+  bta::g_on.store(on != 0);
+  return BTA_OK;
+}
+
+int bta_prof_read(double* ms, long long* counts) {
+  using namespace bta;
+  std::lock_guard<std::mutex> lk(g_mu);
+  for (auto& p : g_pending) {
+    if (cudaEventSynchronize(p.b) != cudaSuccess) return BTA_ERR_CUDA;
+    float t = 0.f;
+    cudaEventElapsedTime(&t, p.a, p.b);
+    g_ms[p.cat] += t;
+    g_cnt[p.cat] += 1;
+    g_pool.push_back(p.a);
+    g_pool.push_back(p.b);
+  }
+  g_pending.clear();
+  for (int i = 0; i < PROF_NCAT; ++i) {
+    if (ms) ms[i] = g_ms[i];
+    if (counts) counts[i] = g_cnt[i];
+    g_ms[i] = 0;
+    g_cnt[i] = 0;
+  }
+  return BTA_OK;
+}
+
+}  // extern "C"

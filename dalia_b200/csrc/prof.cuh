@@ -1,0 +1,23 @@
+// Launch accounting: every kernel launch of the library is counted, and, when
+// enabled, bracketed by CUDA events on its stream so callers can read the
+// device time per kernel category (bta_prof_read in include/dalia_bta.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace bta {
+
+enum ProfCat : int { PROF_PANEL = 0, PROF_GEMM = 1, PROF_SWEEP = 2, PROF_TRTRI = 3, PROF_OTHER = 4, PROF_NCAT = 8 };
+
+void prof_begin(int cat, cudaStream_t s, cudaEvent_t* ev);
+void prof_end(int cat, cudaStream_t s, cudaEvent_t ev);
+
+struct ProfScope {
+  int cat;
+  cudaStream_t s;
+  cudaEvent_t ev = nullptr;
+  ProfScope(int c, cudaStream_t st) : cat(c), s(st) { prof_begin(cat, s, &ev); }
+  ~ProfScope() { prof_end(cat, s, ev); }
+};
+
+}  // namespace bta

@@ -5,6 +5,7 @@
 #include "bta_internal.cuh"
 #include "common.cuh"
 #include "tile_ops.cuh"
+#include "prof.cuh"
 
 namespace bta {
 namespace {
@@ -142,15 +143,24 @@ int block_trtri(const double* D, const double* tile_inv, int i0, int i1, int b, 
   }
   const int nblk = i1 - i0, nq = (b + T - 1) / T;
   if (nblk <= 0) return cudaSuccess;
-  block_trtri_kernel<<<nblk * nq, THREADS, TRTRI_SMEM, s>>>(D, tile_inv, i0, nblk, b, nq, out);
+  {
+    bta::ProfScope _ps(bta::PROF_TRTRI, s);
+    block_trtri_kernel<<<nblk * nq, THREADS, TRTRI_SMEM, s>>>(D, tile_inv, i0, nblk, b, nq, out);
+  }
   return cudaGetLastError();
 }
 
 int logdet_launch(const double* D, int n, int b, const double* Tt, int a, double* part, double* out,
                   cudaStream_t s) {
   const int cnt = n + (a > 0 ? 1 : 0);
-  if (cnt > 0) logdet_part_kernel<<<cnt, 256, 0, s>>>(D, n, b, Tt, a, part);
-  logdet_final_kernel<<<1, 32, 0, s>>>(part, cnt, out);
+  if (cnt > 0) {
+    bta::ProfScope _ps(bta::PROF_OTHER, s);
+    logdet_part_kernel<<<cnt, 256, 0, s>>>(D, n, b, Tt, a, part);
+  }
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, s);
+    logdet_final_kernel<<<1, 32, 0, s>>>(part, cnt, out);
+  }
   return cudaGetLastError();
 }
 

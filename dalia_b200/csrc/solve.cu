@@ -10,6 +10,7 @@
 #include "bta_internal.cuh"
 #include "common.cuh"
 #include "tile_ops.cuh"
+#include "prof.cuh"
 
 namespace bta {
 namespace {
@@ -280,7 +281,10 @@ int diag_tile_inverses(const double* D, int n, int b, double* out, cudaStream_t 
     attr = true;
   }
   if (n * nq == 0) return cudaSuccess;
-  diag_tile_inverse_kernel<<<n * nq, THREADS, smem, s>>>(D, n, b, nq, out);
+  {
+    bta::ProfScope _ps(bta::PROF_SWEEP, s);
+    diag_tile_inverse_kernel<<<n * nq, THREADS, smem, s>>>(D, n, b, nq, out);
+  }
   return cudaGetLastError();
 }
 
@@ -291,20 +295,29 @@ int sweep_launch(const SweepArgs& A, cudaStream_t s) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = std::min(total, sms * 8);
-  sweep_kernel<<<grid, THREADS, 0, s>>>(A);
+  {
+    bta::ProfScope _ps(bta::PROF_SWEEP, s);
+    sweep_kernel<<<grid, THREADS, 0, s>>>(A);
+  }
   return cudaGetLastError();
 }
 
 int arrow_forward(const double* Ab, const double* Tt, double* x, int n, int b, int a, cudaStream_t s) {
   if (a <= 0) return cudaSuccess;
   const size_t smem = (size_t)(a + 256) * sizeof(double);
-  arrow_forward_kernel<<<1, 256, smem, s>>>(Ab, Tt, x, n, b, a);
+  {
+    bta::ProfScope _ps(bta::PROF_SWEEP, s);
+    arrow_forward_kernel<<<1, 256, smem, s>>>(Ab, Tt, x, n, b, a);
+  }
   return cudaGetLastError();
 }
 
 int arrow_backward(const double* Tt, double* x, int n, int b, int a, cudaStream_t s) {
   if (a <= 0) return cudaSuccess;
-  arrow_backward_kernel<<<1, 32, 0, s>>>(Tt, x, (long long)n * b, a);
+  {
+    bta::ProfScope _ps(bta::PROF_SWEEP, s);
+    arrow_backward_kernel<<<1, 32, 0, s>>>(Tt, x, (long long)n * b, a);
+  }
   return cudaGetLastError();
 }
 

@@ -113,6 +113,19 @@ int bta_gather_coo(bta_handle_t h, int64_t n, int64_t b, int64_t a, const int64_
                    int64_t nnz, int sparsity_bt, const double* D, const double* L, const double* Ab, const double* T,
                    double* out);
 
+/*
+ * Launch accounting (no counterpart in the reference, which has no native
+ * kernels): total kernel launches of this library in the process, and
+ * optional per-category device time from CUDA events recorded around every
+ * launch on its stream.  Categories: 0 panel factorisation, 1 GEMM, 2 solve
+ * sweeps, 3 block inverses, 4 other.  bta_prof_read synchronises on the
+ * recorded events, returns the accumulated milliseconds and launch counts
+ * (8 entries each) and clears them.
+ */
+long long bta_launch_count(void);
+int bta_prof_enable(int on);
+int bta_prof_read(double* ms, long long* counts);
+
 #ifdef __cplusplus
 }
 #endif
