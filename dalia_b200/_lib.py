@@ -42,6 +42,8 @@ SIGNATURES = {
     "bta_get_status": (_int, [_c_void_p, _pi64]),
     "bta_reset_status": (_int, [_c_void_p]),
     "bta_launch_count": (ctypes.c_longlong, []),
+    "bta_pobtaf_noalloc": (_int, [_i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _pi64, _c_void_p]),
+    "bta_noalloc_scratch_bytes": (ctypes.c_size_t, []),
     "bta_prof_enable": (_int, [_int]),
     "bta_prof_read": (_int, [_pdbl, ctypes.POINTER(ctypes.c_longlong)]),
     "bta_gather_coo": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _i64, _int,
