@@ -37,6 +37,10 @@ SIGNATURES = {
     "bta_workspace_bytes": (ctypes.c_size_t, [_c_void_p]),
     "bta_pobtaf": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _pi64]),
     "bta_pobtas": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _int]),
+    "bta_pobtaf_batched": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                  _c_void_p, _pi64]),
+    "bta_pobtasi_batched": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                   _c_void_p, _c_void_p]),
     "bta_pobtasi": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p]),
     "bta_logdet": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _int, _c_void_p, _pdbl]),
     "bta_get_status": (_int, [_c_void_p, _pi64]),

@@ -22,7 +22,7 @@ struct bta_context {
   size_t ws_bytes = 0;
   int* ctl = nullptr;  // [0] abort flag, [1] scratch; ctl+2 (8-aligned): info (u64)
   double* scal = nullptr;
-  std::map<std::tuple<int, int, int>, std::pair<int4*, int>> tasks;
+  std::map<std::vector<int>, std::pair<int4*, int>> tasks;
 };
 
 namespace {
@@ -63,22 +63,36 @@ inline unsigned long long* info_ptr(bta_context* h) { return reinterpret_cast<un
 int cuda_rc(cudaError_t e) { return e == cudaSuccess ? BTA_OK : BTA_ERR_CUDA; }
 int cuda_rc(int e) { return e == 0 ? BTA_OK : BTA_ERR_CUDA; }
 
-// Cached device task list of a single-instance panel.
-int get_tasks(bta_context* h, int b, int a, bool hasL, const int4** out, int* count) {
-  auto key = std::make_tuple(b, a, hasL ? 1 : 0);
+// One instance of a batched panel launch.
+struct PanelSpec {
+  double* D;
+  double* L;
+  double* Ab;
+  int b, a;
+  long long base;
+  const double* Lprev = nullptr;
+  const double* Abprev = nullptr;
+  double* Ttip = nullptr;
+};
+
+// Cached device task list of a panel batch with the given instance shapes.
+int get_tasks(bta_context* h, const std::vector<PanelInst>& insts, const int4** out, int* count) {
+  std::vector<int> key;
+  for (const auto& I : insts) {
+    key.push_back(I.b);
+    key.push_back(I.a);
+    key.push_back((I.L != nullptr ? 1 : 0) | (I.Ttip != nullptr ? 2 : 0));
+  }
   auto it = h->tasks.find(key);
   if (it == h->tasks.end()) {
-    PanelInst I{};
-    I.b = b;
-    I.a = a;
-    I.nq = (b + 63) / 64;
-    I.L = hasL ? reinterpret_cast<double*>(1) : nullptr;
-    I.nrows_t = panel_rows(b, a, hasL);
     std::vector<int4> t;
-    panel_tasks({I}, t);
+    panel_tasks(insts, t);
     int4* d = nullptr;
-    if (cudaMalloc(&d, t.size() * sizeof(int4)) != cudaSuccess) return BTA_ERR_ALLOC;
-    if (cudaMemcpy(d, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess) return BTA_ERR_CUDA;
+    if (!t.empty()) {
+      if (cudaMalloc(&d, t.size() * sizeof(int4)) != cudaSuccess) return BTA_ERR_ALLOC;
+      if (cudaMemcpy(d, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess)
+        return BTA_ERR_CUDA;
+    }
     it = h->tasks.emplace(key, std::make_pair(d, (int)t.size())).first;
   }
   *out = it->second.first;
@@ -86,40 +100,58 @@ int get_tasks(bta_context* h, int b, int a, bool hasL, const int4** out, int* co
   return BTA_OK;
 }
 
-// Factor one panel (diag block D, optional L below, optional arrow rows Ab).
-int run_panel(bta_context* h, double* D, double* L, double* Ab, int b, int a, long long base, Carve& cv) {
-  const bool hasL = L != nullptr;
-  const int aa = Ab != nullptr ? a : 0;
-  const int nq = (b + 63) / 64;
-  const int nr = panel_rows(b, aa, hasL);
-  double* linv = cv.take<double>((size_t)nq * 64 * 64);
-  int* cnt = cv.take<int>((size_t)2 * nr * nq + 4);
-  const int4* tasks;
-  int ntasks;
-  int rc = get_tasks(h, b, aa, hasL, &tasks, &ntasks);
-  if (rc) return rc;
-  if (cudaMemsetAsync(cnt, 0, ((size_t)2 * nr * nq + 4) * sizeof(int), h->stream) != cudaSuccess) return BTA_ERR_CUDA;
-  PanelBatch B;
-  std::memset(&B, 0, sizeof(B));
-  B.ninst = 1;
-  B.ntasks = ntasks;
-  B.tasks = tasks;
-  B.counter = cnt + 2 * nr * nq;
-  B.abort_flag = h->ctl;
-  PanelInst& I = B.inst[0];
-  I.D = D;
-  I.L = L;
-  I.Ab = aa ? Ab : nullptr;
-  I.Linv = linv;
-  I.upd = cnt;
-  I.flag = cnt + nr * nq;
-  I.info = info_ptr(h);
-  I.pivot_base = base;
-  I.b = b;
-  I.a = aa;
-  I.nq = nq;
-  I.nrows_t = nr;
-  return cuda_rc(panel_launch(B, 0, h->stream));
+// Factor one block column of every instance in one launch (chunks of
+// PANEL_MAXI instances).
+int run_panels(bta_context* h, const std::vector<PanelSpec>& specs, Carve& cv) {
+  for (size_t c0 = 0; c0 < specs.size(); c0 += PANEL_MAXI) {
+    const size_t c1 = std::min(specs.size(), c0 + (size_t)PANEL_MAXI);
+    PanelBatch B;
+    std::memset(&B, 0, sizeof(B));
+    std::vector<PanelInst> insts;
+    size_t cnt_total = 0;
+    for (size_t k = c0; k < c1; ++k) {
+      const PanelSpec& sp = specs[k];
+      const bool hasL = sp.L != nullptr;
+      const int aa = sp.Ab != nullptr ? sp.a : 0;
+      PanelInst I{};
+      I.D = sp.D;
+      I.L = sp.L;
+      I.Ab = aa ? sp.Ab : nullptr;
+      I.b = sp.b;
+      I.a = aa;
+      I.nq = (sp.b + 63) / 64;
+      I.nrows_t = panel_rows(sp.b, aa, hasL);
+      I.pivot_base = sp.base;
+      I.info = info_ptr(h);
+      I.Lprev = sp.Lprev;
+      I.Abprev = aa ? sp.Abprev : nullptr;
+      I.Ttip = (aa > 0 && aa <= 64) ? sp.Ttip : nullptr;
+      I.Linv = cv.take<double>((size_t)I.nq * 64 * 64);
+      cnt_total += (size_t)2 * I.nrows_t * I.nq;
+      insts.push_back(I);
+    }
+    int* cnt = cv.take<int>(cnt_total + 4);
+    size_t off = 0;
+    for (auto& I : insts) {
+      I.upd = cnt + off;
+      I.flag = cnt + off + (size_t)I.nrows_t * I.nq;
+      off += (size_t)2 * I.nrows_t * I.nq;
+    }
+    const int4* tasks;
+    int ntasks;
+    int rc = get_tasks(h, insts, &tasks, &ntasks);
+    if (rc) return rc;
+    if (cudaMemsetAsync(cnt, 0, (cnt_total + 4) * sizeof(int), h->stream) != cudaSuccess) return BTA_ERR_CUDA;
+    B.ninst = (int)insts.size();
+    B.ntasks = ntasks;
+    B.tasks = tasks;
+    B.counter = cnt + cnt_total;
+    B.abort_flag = h->ctl;
+    for (size_t k = 0; k < insts.size(); ++k) B.inst[k] = insts[k];
+    rc = cuda_rc(panel_launch(B, 0, h->stream));
+    if (rc) return rc;
+  }
+  return BTA_OK;
 }
 
 size_t panel_ws_bytes(int b, int a) {
@@ -232,52 +264,74 @@ int bta_set_stream(bta_handle_t h, void* stream) {
 
 size_t bta_workspace_bytes(bta_handle_t h) { return h ? h->ws_bytes : 0; }
 
-int bta_pobtaf(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, double* L, double* Ab, double* T,
-               int64_t* info) {
-  if (!h || n < 1 || b < 1 || a < 0 || !D || (n > 1 && !L) || (a > 0 && (!Ab || !T))) return BTA_ERR_INVALID;
-  if (b > 65535 * 64 || a > 4096) return BTA_ERR_INVALID;
-  const size_t need = panel_ws_bytes((int)b, (int)a) + (a > 0 ? panel_ws_bytes((int)a, 0) : 0);
-  int rc = ensure_ws(h, need);
+int bta_pobtaf_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                       double* const* D, double* const* L, double* const* Ab, double* const* T, int64_t* info) {
+  if (!h || count < 1 || !n || !b || !a || !D) return BTA_ERR_INVALID;
+  int64_t maxn = 0;
+  size_t need = 0, need_tip = 0;
+  for (int k = 0; k < count; ++k) {
+    if (n[k] < 1 || b[k] < 1 || a[k] < 0 || !D[k] || (n[k] > 1 && (!L || !L[k])) ||
+        (a[k] > 0 && (!Ab || !T || !Ab[k] || !T[k])))
+      return BTA_ERR_INVALID;
+    if (b[k] > 65535 || a[k] > 4096) return BTA_ERR_INVALID;
+    maxn = std::max(maxn, n[k]);
+    need += panel_ws_bytes((int)b[k], (int)a[k]);
+    if (a[k] > 0) need_tip += panel_ws_bytes((int)a[k], 0);
+  }
+  int rc = ensure_ws(h, std::max(need, need_tip) + 4 * kAlign);
   if (rc) return rc;
   cudaStream_t s = h->stream;
   if (info) {
     rc = reset_status(h);
     if (rc) return rc;
   }
-  const size_t bb = (size_t)b * b, ab = (size_t)a * b;
-  for (int64_t i = 0; i < n; ++i) {
-    const bool hasL = i < n - 1;
-    double* Di = D + i * bb;
-    double* Li = hasL ? L + i * bb : nullptr;
-    double* Abi = a > 0 ? Ab + i * ab : nullptr;
-    Carve cv{h->ws};
-    rc = run_panel(h, Di, Li, Abi, (int)b, (int)a, (long long)(i * b), cv);
-    if (rc) return rc;
+  // pivot index of instance k: k * 2^40 + global row (1-based).  Each launch
+  // factors block column i and applies block column i-1's Schur update to it.
+  for (int64_t i = 0; i < maxn; ++i) {
+    std::vector<PanelSpec> specs;
     std::vector<GemmProb> probs;
-    if (hasL) {
-      GemmProb p = gemm_prob(D + (i + 1) * bb, (int)b, (int)b, (int)b, 1.0, GC_LOWER);
-      gemm_add(p, Li, (int)b, Li, (int)b, (int)b, -1.0, 0);
-      probs.push_back(p);
-    }
-    if (a > 0) {
-      if (hasL) {
-        GemmProb p = gemm_prob(Ab + (i + 1) * ab, (int)b, (int)a, (int)b, 1.0);
-        gemm_add(p, Abi, (int)b, Li, (int)b, (int)b, -1.0, 0);
+    for (int k = 0; k < count; ++k) {
+      if (i >= n[k]) continue;
+      const size_t bb = (size_t)b[k] * b[k], ab = (size_t)a[k] * b[k];
+      const bool hasL = i < n[k] - 1;
+      double* Di = D[k] + i * bb;
+      double* Li = hasL ? L[k] + i * bb : nullptr;
+      double* Abi = a[k] > 0 ? Ab[k] + i * ab : nullptr;
+      PanelSpec sp{Di, Li, Abi, (int)b[k], (int)a[k], ((long long)k << 40) + (long long)(i * b[k])};
+      if (i > 0) {
+        sp.Lprev = L[k] + (i - 1) * bb;
+        sp.Abprev = a[k] > 0 ? Ab[k] + (i - 1) * ab : nullptr;
+      }
+      sp.Ttip = a[k] > 0 ? T[k] : nullptr;
+      specs.push_back(sp);
+      if (a[k] > 64) {  // the in-panel tip task covers one arrow tile row
+        const int B_ = (int)b[k], A_ = (int)a[k];
+        GemmProb p = gemm_prob(T[k], A_, A_, A_, 1.0);
+        gemm_add(p, Abi, B_, Abi, B_, B_, -1.0, 0);
         probs.push_back(p);
       }
-      GemmProb p = gemm_prob(T, (int)a, (int)a, (int)a, 1.0);
-      gemm_add(p, Abi, (int)b, Abi, (int)b, (int)b, -1.0, 0);
-      probs.push_back(p);
     }
+    Carve cv{h->ws};
+    rc = run_panels(h, specs, cv);
+    if (rc) return rc;
     if (!probs.empty() && gemm_launch(probs, s) != cudaSuccess) return BTA_ERR_CUDA;
   }
-  if (a > 0) {
+  std::vector<PanelSpec> tips;
+  for (int k = 0; k < count; ++k)
+    if (a[k] > 0) tips.push_back({T[k], nullptr, nullptr, (int)a[k], 0, ((long long)k << 40) + (long long)(n[k] * b[k])});
+  if (!tips.empty()) {
     Carve cv{h->ws};
-    rc = run_panel(h, T, nullptr, nullptr, (int)a, 0, (long long)(n * b), cv);
+    rc = run_panels(h, tips, cv);
     if (rc) return rc;
   }
   if (info) return check_status(h, info);
   return cuda_rc(cudaGetLastError());
+}
+
+int bta_pobtaf(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, double* L, double* Ab, double* T,
+               int64_t* info) {
+  if (!h || n < 1 || b < 1 || a < 0 || !D || (n > 1 && !L) || (a > 0 && (!Ab || !T))) return BTA_ERR_INVALID;
+  return bta_pobtaf_batched(h, 1, &n, &b, &a, &D, &L, &Ab, &T, info);
 }
 
 int bta_pobtas(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D, const double* L,
@@ -318,74 +372,107 @@ int bta_pobtas(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D,
   return cuda_rc(cudaGetLastError());
 }
 
-int bta_pobtasi(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, double* L, double* Ab, double* T) {
-  if (!h || n < 1 || b < 1 || a < 0 || !D || (n > 1 && !L) || (a > 0 && (!Ab || !T))) return BTA_ERR_INVALID;
-  const int nq = (int)((b + 63) / 64);
-  const int nqa = (int)((a + 63) / 64);
-  const size_t bb = (size_t)b * b, ab = (size_t)a * b;
-  const size_t need = align_up((size_t)n * nq * 4096 * 8) + align_up((size_t)n * bb * 8) + 2 * align_up(bb * 8) +
-                      align_up(ab * 8 + 8) + align_up((size_t)nqa * 4096 * 8 + 8) + align_up((size_t)a * a * 8 + 8) +
-                      8 * kAlign;
+int bta_pobtasi_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                        double* const* D, double* const* L, double* const* Ab, double* const* T) {
+  if (!h || count < 1 || !n || !b || !a || !D) return BTA_ERR_INVALID;
+  size_t need = 8 * kAlign;
+  int64_t maxn = 0;
+  for (int k = 0; k < count; ++k) {
+    if (n[k] < 1 || b[k] < 1 || a[k] < 0 || !D[k] || (n[k] > 1 && (!L || !L[k])) ||
+        (a[k] > 0 && (!Ab || !T || !Ab[k] || !T[k])))
+      return BTA_ERR_INVALID;
+    const size_t nq = (b[k] + 63) / 64, nqa = (a[k] + 63) / 64;
+    const size_t bb = (size_t)b[k] * b[k], ab = (size_t)a[k] * b[k];
+    need += align_up(n[k] * nq * 4096 * 8) + align_up(n[k] * bb * 8) + 2 * align_up(bb * 8) + align_up(ab * 8 + 8) +
+            align_up(nqa * 4096 * 8 + 8) + align_up((size_t)a[k] * a[k] * 8 + 8) + 7 * kAlign;
+    maxn = std::max(maxn, n[k]);
+  }
   int rc = ensure_ws(h, need);
   if (rc) return rc;
   cudaStream_t s = h->stream;
   Carve cv{h->ws};
-  double* tinv = cv.take<double>((size_t)n * nq * 4096);
-  double* Linv = cv.take<double>((size_t)n * bb);
-  double* G = cv.take<double>(bb);
-  double* S = cv.take<double>(bb);
-  double* Ga = cv.take<double>(ab + 1);
-  double* tinv_t = cv.take<double>((size_t)nqa * 4096 + 1);
-  double* Wt = cv.take<double>((size_t)a * a + 1);
-  if (diag_tile_inverses(D, (int)n, (int)b, tinv, s)) return BTA_ERR_CUDA;
-  if (block_trtri(D, tinv, 0, (int)n, (int)b, Linv, s)) return BTA_ERR_CUDA;
-  if (a > 0) {
-    if (diag_tile_inverses(T, 1, (int)a, tinv_t, s)) return BTA_ERR_CUDA;
-    if (block_trtri(T, tinv_t, 0, 1, (int)a, Wt, s)) return BTA_ERR_CUDA;
-    GemmProb p = gemm_prob(T, (int)a, (int)a, (int)a, 0.0, GC_LOWER | GC_MIRROR);
-    gemm_add(p, Wt, (int)a, Wt, (int)a, (int)a, 1.0, GF_A_T | GF_B_KN | GF_K_GE_M | GF_K_GE_N);
-    if (gemm_launch({p}, s)) return BTA_ERR_CUDA;
+  struct W {
+    double *tinv, *Linv, *G, *S, *Ga, *tinv_t, *Wt;
+  };
+  std::vector<W> w(count);
+  for (int k = 0; k < count; ++k) {
+    const size_t nq = (b[k] + 63) / 64, nqa = (a[k] + 63) / 64;
+    const size_t bb = (size_t)b[k] * b[k], ab = (size_t)a[k] * b[k];
+    w[k].tinv = cv.take<double>(n[k] * nq * 4096);
+    w[k].Linv = cv.take<double>(n[k] * bb);
+    w[k].G = cv.take<double>(bb);
+    w[k].S = cv.take<double>(bb);
+    w[k].Ga = cv.take<double>(ab + 1);
+    w[k].tinv_t = cv.take<double>(nqa * 4096 + 1);
+    w[k].Wt = cv.take<double>((size_t)a[k] * a[k] + 1);
   }
-  for (int64_t i = n - 1; i >= 0; --i) {
-    const bool hasL = i < n - 1;
-    double* Di = D + i * bb;
-    double* Li = hasL ? L + i * bb : nullptr;
-    double* Abi = a > 0 ? Ab + i * ab : nullptr;
-    const double* Vi = Linv + i * bb;
-    const int B_ = (int)b, A_ = (int)a;
-    std::vector<GemmProb> pa, pb;
-    if (hasL) {
-      GemmProb p = gemm_prob(G, B_, B_, B_, 0.0);
-      gemm_add(p, Li, B_, Vi, B_, B_, 1.0, GF_B_KN | GF_K_GE_N);
-      pa.push_back(p);
+  std::vector<GemmProb> ptip;
+  for (int k = 0; k < count; ++k) {
+    if (diag_tile_inverses(D[k], (int)n[k], (int)b[k], w[k].tinv, s)) return BTA_ERR_CUDA;
+    if (block_trtri(D[k], w[k].tinv, 0, (int)n[k], (int)b[k], w[k].Linv, s)) return BTA_ERR_CUDA;
+    if (a[k] > 0) {
+      const int A_ = (int)a[k];
+      if (diag_tile_inverses(T[k], 1, A_, w[k].tinv_t, s)) return BTA_ERR_CUDA;
+      if (block_trtri(T[k], w[k].tinv_t, 0, 1, A_, w[k].Wt, s)) return BTA_ERR_CUDA;
+      GemmProb p = gemm_prob(T[k], A_, A_, A_, 0.0, GC_LOWER | GC_MIRROR);
+      gemm_add(p, w[k].Wt, A_, w[k].Wt, A_, A_, 1.0, GF_A_T | GF_B_KN | GF_K_GE_M | GF_K_GE_N);
+      ptip.push_back(p);
     }
-    if (a > 0) {
-      GemmProb p = gemm_prob(Ga, B_, A_, B_, 0.0);
-      gemm_add(p, Abi, B_, Vi, B_, B_, 1.0, GF_B_KN | GF_K_GE_N);
-      pa.push_back(p);
+  }
+  if (!ptip.empty() && gemm_launch(ptip, s)) return BTA_ERR_CUDA;
+  // step st processes block j = n_k - 1 - st of every instance
+  for (int64_t st = 0; st < maxn; ++st) {
+    std::vector<GemmProb> pa, pb, pc;
+    for (int k = 0; k < count; ++k) {
+      const int64_t i = n[k] - 1 - st;
+      if (i < 0) continue;
+      const size_t bb = (size_t)b[k] * b[k], ab = (size_t)a[k] * b[k];
+      const bool hasL = i < n[k] - 1;
+      double* Li = hasL ? L[k] + i * bb : nullptr;
+      double* Abi = a[k] > 0 ? Ab[k] + i * ab : nullptr;
+      const double* Vi = w[k].Linv + i * bb;
+      const int B_ = (int)b[k], A_ = (int)a[k];
+      if (hasL) {
+        GemmProb p = gemm_prob(w[k].G, B_, B_, B_, 0.0);
+        gemm_add(p, Li, B_, Vi, B_, B_, 1.0, GF_B_KN | GF_K_GE_N);
+        pa.push_back(p);
+        GemmProb q = gemm_prob(Li, B_, B_, B_, 0.0);
+        gemm_add(q, D[k] + (i + 1) * bb, B_, w[k].G, B_, B_, -1.0, GF_B_KN);
+        if (a[k] > 0) gemm_add(q, Ab[k] + (i + 1) * ab, B_, w[k].Ga, B_, A_, -1.0, GF_A_T | GF_B_KN);
+        pb.push_back(q);
+      }
+      if (a[k] > 0) {
+        GemmProb p = gemm_prob(w[k].Ga, B_, A_, B_, 0.0);
+        gemm_add(p, Abi, B_, Vi, B_, B_, 1.0, GF_B_KN | GF_K_GE_N);
+        pa.push_back(p);
+        GemmProb q = gemm_prob(Abi, B_, A_, B_, 0.0);
+        if (hasL) gemm_add(q, Ab[k] + (i + 1) * ab, B_, w[k].G, B_, B_, -1.0, GF_B_KN);
+        gemm_add(q, T[k], A_, w[k].Ga, B_, A_, -1.0, GF_B_KN);
+        pb.push_back(q);
+      }
+      GemmProb r = gemm_prob(w[k].S, B_, B_, B_, 0.0, GC_LOWER | GC_MIRROR);
+      gemm_add(r, Vi, B_, Vi, B_, B_, 1.0, GF_A_T | GF_B_KN | GF_K_GE_M | GF_K_GE_N);
+      if (hasL) gemm_add(r, w[k].G, B_, Li, B_, B_, -1.0, GF_A_T | GF_B_KN);
+      if (a[k] > 0) gemm_add(r, w[k].Ga, B_, Abi, B_, A_, -1.0, GF_A_T | GF_B_KN);
+      pc.push_back(r);
     }
     if (!pa.empty() && gemm_launch(pa, s)) return BTA_ERR_CUDA;
-    if (hasL) {
-      GemmProb p = gemm_prob(Li, B_, B_, B_, 0.0);
-      gemm_add(p, D + (i + 1) * bb, B_, G, B_, B_, -1.0, GF_B_KN);
-      if (a > 0) gemm_add(p, Ab + (i + 1) * ab, B_, Ga, B_, A_, -1.0, GF_A_T | GF_B_KN);
-      pb.push_back(p);
-    }
-    if (a > 0) {
-      GemmProb p = gemm_prob(Abi, B_, A_, B_, 0.0);
-      if (hasL) gemm_add(p, Ab + (i + 1) * ab, B_, G, B_, B_, -1.0, GF_B_KN);
-      gemm_add(p, T, A_, Ga, B_, A_, -1.0, GF_B_KN);
-      pb.push_back(p);
-    }
     if (!pb.empty() && gemm_launch(pb, s)) return BTA_ERR_CUDA;
-    GemmProb pc = gemm_prob(S, B_, B_, B_, 0.0, GC_LOWER | GC_MIRROR);
-    gemm_add(pc, Vi, B_, Vi, B_, B_, 1.0, GF_A_T | GF_B_KN | GF_K_GE_M | GF_K_GE_N);
-    if (hasL) gemm_add(pc, G, B_, Li, B_, B_, -1.0, GF_A_T | GF_B_KN);
-    if (a > 0) gemm_add(pc, Ga, B_, Abi, B_, A_, -1.0, GF_A_T | GF_B_KN);
-    if (gemm_launch({pc}, s)) return BTA_ERR_CUDA;
-    if (cudaMemcpyAsync(Di, S, bb * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess) return BTA_ERR_CUDA;
+    if (!pc.empty() && gemm_launch(pc, s)) return BTA_ERR_CUDA;
+    for (int k = 0; k < count; ++k) {
+      const int64_t i = n[k] - 1 - st;
+      if (i < 0) continue;
+      const size_t bb = (size_t)b[k] * b[k];
+      if (cudaMemcpyAsync(D[k] + i * bb, w[k].S, bb * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        return BTA_ERR_CUDA;
+    }
   }
   return cuda_rc(cudaGetLastError());
+}
+
+int bta_pobtasi(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, double* L, double* Ab, double* T) {
+  if (!h || n < 1 || b < 1 || a < 0 || !D || (n > 1 && !L) || (a > 0 && (!Ab || !T))) return BTA_ERR_INVALID;
+  return bta_pobtasi_batched(h, 1, &n, &b, &a, &D, &L, &Ab, &T);
 }
 
 int bta_logdet(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D, const double* T, int include_tip,

@@ -81,6 +81,39 @@ __device__ __forceinline__ TileRef tile_of(const PanelInst& I, int p, int c) {
   return t;
 }
 
+
+// Tile (p, c) of the previous block column's sub-diagonal and arrow blocks:
+// rows of this panel's diagonal block read L_prev, arrow rows read Ab_prev;
+// rows of the block below have no previous-step term (returns rows = 0).
+__device__ __forceinline__ TileRef prev_tile_of(const PanelInst& I, int p, int c) {
+  TileRef t;
+  t.cols = min(T, I.b - c * T);
+  if (p < I.nq) {
+    t.ptr = const_cast<double*>(I.Lprev) + (size_t)(p * T) * I.b + c * T;
+    t.rows = min(T, I.b - p * T);
+  } else if (I.L != nullptr && p < 2 * I.nq) {
+    t.ptr = nullptr;
+    t.rows = 0;
+  } else {
+    const int ar = p - I.nq - (I.L != nullptr ? I.nq : 0);
+    t.ptr = const_cast<double*>(I.Abprev) + (size_t)(ar * T) * I.b + c * T;
+    t.rows = min(T, I.a - ar * T);
+  }
+  return t;
+}
+
+// acc += X Y^T for two global tiles (staged through the two smem buffers).
+__device__ __forceinline__ void acc_pair(const TileRef& x, const TileRef& y, double* bufA, double* bufL, int ld,
+                                         double (&acc)[2][4][4], int tid, int wm, int wn, int g, int t) {
+  load_async<SG>(bufA, x.ptr, ld, x.rows, x.cols, tid);
+  load_async<SG>(bufL, y.ptr, ld, y.rows, y.cols, tid);
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  mma_nt(bufA, bufL, (x.cols + 3) & ~3, acc, wm, wn, g, t);
+  __syncthreads();
+}
+
 // Block-wide wait by thread 0; returns the verdict to every thread.
 __device__ __forceinline__ bool block_wait(const int* p, int target, int* abort_flag, int* s_ok) {
   if (threadIdx.x == 0) *s_ok = wait_ge(p, target, abort_flag) ? 1 : 0;
@@ -111,7 +144,7 @@ __device__ void run_chain(const PanelInst& I, double* bufA, double* bufL, double
     const int w = d.cols;
     TRACE_T0();
     if (q > 0) {
-      if (!block_wait(&I.upd[q * nq + q - 1], q - 1, abort_flag, s_ok)) return;
+      if (!block_wait(&I.upd[q * nq + q - 1], 1, abort_flag, s_ok)) return;
       const TileRef x = tile_of(I, q, q - 1);
       load_async<SG>(Wk, x.ptr, ld, x.rows, x.cols, tid);
       cp_async_commit();
@@ -137,7 +170,7 @@ __device__ void run_chain(const PanelInst& I, double* bufA, double* bufL, double
             }
         }
       release(&I.flag[q * nq + q - 1], 1);
-      if (!block_wait(&I.upd[q * nq + q], q - 1, abort_flag, s_ok)) return;
+      if (!block_wait(&I.upd[q * nq + q], 1, abort_flag, s_ok)) return;
       TRACE_T1();
       TRACE(8, q, 0);
       zero_acc(acc);
@@ -160,6 +193,7 @@ __device__ void run_chain(const PanelInst& I, double* bufA, double* bufL, double
         }
       __syncthreads();
     } else {
+      if (!block_wait(&I.upd[0], 1, abort_flag, s_ok)) return;
       load<SG>(Lv, d.ptr, ld, w, w, tid);
       __syncthreads();
     }
@@ -178,14 +212,6 @@ __device__ void run_chain(const PanelInst& I, double* bufA, double* bufL, double
       const double li = in ? Wk[i * SG + k] : 0.0;
       linv[idx] = li;
       Wk[i * SG + k] = li;  // zero-padded operand for the next step
-    }
-    // strictly-upper tiles of this tile column become zero (LAPACK-style factor)
-    for (int qq = 0; qq < q; ++qq) {
-      double* up = I.D + (size_t)(qq * T) * ld + q * T;
-      for (int idx = tid; idx < T * T; idx += THREADS) {
-        const int i = idx >> 6, k = idx & 63;
-        if (k < w) up[(size_t)i * ld + k] = 0.0;
-      }
     }
     double* tmp = Lv;
     Lv = Wk;
@@ -219,74 +245,76 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
     if (ti >= B.ntasks) break;
     const int4 tk = B.tasks[ti];
     const PanelInst& I = B.inst[tk.x];
-    const int kind = tk.y, p = tk.z, r = tk.w >> 16, q = tk.w & 0xffff;
+    const int kind = tk.y, p = tk.z, r = tk.w;
     const int nq = I.nq, ld = I.b;
     TRACE_T0();
-    if (tid == 0) {
-      bool ok;
-      if (kind == TASK_TRSM) {
-        ok = wait_ge(&I.flag[q * nq + q], 1, B.abort_flag) && wait_ge(&I.upd[p * nq + q], q, B.abort_flag);
-      } else {
-        ok = wait_ge(&I.flag[p * nq + q], 1, B.abort_flag) && wait_ge(&I.flag[r * nq + q], 1, B.abort_flag) &&
-             wait_ge(&I.upd[p * nq + r], q, B.abort_flag);
-      }
-      s_ok = ok ? 1 : 0;
-    }
-    __syncthreads();
-    if (!s_ok) continue;
-    TRACE_T1();
-
+    // left-looking accumulation of tile(p, r) -= sum_k X(p, k) X(r, k)^T:
+    // first the previous block column's terms (final before this launch),
+    // then this panel's columns as they become final
     double acc[2][4][4];
     zero_acc(acc);
-    if (kind == TASK_TRSM) {
-      const TileRef x = tile_of(I, p, q);
-      load_async<SG>(bufA, x.ptr, ld, x.rows, x.cols, tid);
-      load_async<SG>(bufL, I.Linv + (size_t)q * T * T, T, T, T, tid);
-      cp_async_commit();
-      cp_async_wait<0>();
-      __syncthreads();
-      mma_nt(bufA, bufL, (x.cols + 3) & ~3, acc, wm, wn, g, t);
+    if (kind == TASK_TIP) {
+      // T -= sum_k X(arrow, k) X(arrow, k)^T once the arrow row is final
+      const int pa = I.nrows_t - 1;
+      bool okt = true;
+      for (int k = 0; k < nq && okt; ++k) {
+        if (tid == 0) s_ok = wait_ge(&I.flag[pa * nq + k], 1, B.abort_flag) ? 1 : 0;
+        __syncthreads();
+        okt = s_ok != 0;
+        if (okt) {
+          const TileRef xa = tile_of(I, pa, k);
+          acc_pair(xa, xa, bufA, bufL, ld, acc, tid, wm, wn, g, t);
+        }
+      }
+      if (!okt) continue;
 #pragma unroll
       for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           const int row = wm * 32 + mi * 16 + g + h * 8;
-          if (row >= x.rows) continue;
+          if (row >= I.a) continue;
 #pragma unroll
           for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
               const int col = wn * 32 + ni * 8 + 2 * t + e;
-              if (col < x.cols) x.ptr[(size_t)row * ld + col] = acc[mi][ni][h * 2 + e];
+              if (col < I.a) I.Ttip[row * I.a + col] -= acc[mi][ni][h * 2 + e];
             }
         }
-      release(&I.flag[p * nq + q], 1);
-      TRACE(kind, p, q);
-    } else {
-      const TileRef xp = tile_of(I, p, q);
-      const TileRef xr = tile_of(I, r, q);
-      const TileRef c = tile_of(I, p, r);
-      load_async<SG>(bufA, xp.ptr, ld, xp.rows, xp.cols, tid);
-      load_async<SG>(bufL, xr.ptr, ld, xr.rows, xr.cols, tid);
-      cp_async_commit();
-      // prefetch the destination fragments while the operands land
-      double cv[2][2][4][2];
-#pragma unroll
-      for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int row = wm * 32 + mi * 16 + g + h * 8;
-#pragma unroll
-          for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-              const int col = wn * 32 + ni * 8 + 2 * t + e;
-              cv[mi][h][ni][e] = (row < c.rows && col < c.cols) ? __ldcg(c.ptr + (size_t)row * ld + col) : 0.0;
-            }
-        }
-      cp_async_wait<0>();
+      continue;
+    }
+    if (I.Lprev != nullptr) {
+      const TileRef yp0 = prev_tile_of(I, r, 0);
+      if (prev_tile_of(I, p, 0).rows > 0 && yp0.rows > 0) {
+        for (int k = 0; k < nq; ++k) acc_pair(prev_tile_of(I, p, k), prev_tile_of(I, r, k), bufA, bufL, ld, acc, tid,
+                                              wm, wn, g, t);
+      }
+    }
+    // zero the mirrored strictly-upper tile (r, p) of the diagonal block
+    if (p < nq && p > r) {
+      double* up = I.D + (size_t)(r * T) * ld + p * T;
+      const int cw = min(T, I.b - p * T);
+      for (int idx = tid; idx < T * T; idx += THREADS) {
+        const int i = idx >> 6, k = idx & 63;
+        if (k < cw) up[(size_t)i * ld + k] = 0.0;
+      }
+    }
+    const int kmax = (kind == TASK_AGG_DIAG) ? r - 1 : r;
+    bool ok = true;
+    for (int k = 0; k < kmax && ok; ++k) {
+      if (tid == 0)
+        s_ok = (wait_ge(&I.flag[p * nq + k], 1, B.abort_flag) && wait_ge(&I.flag[r * nq + k], 1, B.abort_flag)) ? 1
+                                                                                                                : 0;
       __syncthreads();
-      mma_nt(bufA, bufL, (xp.cols + 3) & ~3, acc, wm, wn, g, t);
+      ok = s_ok != 0;
+      if (!ok) break;
+      acc_pair(tile_of(I, p, k), tile_of(I, r, k), bufA, bufL, ld, acc, tid, wm, wn, g, t);
+    }
+    if (!ok) continue;
+    TRACE_T1();
+    const TileRef c = tile_of(I, p, r);
+    if (kind != TASK_AGG_TRSM) {
+      // chain input: write the accumulated tile, the chain CTA finishes it
 #pragma unroll
       for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -298,12 +326,57 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
               const int col = wn * 32 + ni * 8 + 2 * t + e;
-              if (col < c.cols) c.ptr[(size_t)row * ld + col] = cv[mi][h][ni][e] - acc[mi][ni][h * 2 + e];
+              if (col < c.cols) {
+                double* dst = c.ptr + (size_t)row * ld + col;
+                *dst = __ldcg(dst) - acc[mi][ni][h * 2 + e];
+              }
             }
         }
-      release(&I.upd[p * nq + r], q + 1);
-      TRACE(kind, p, (r << 8) | q);
+      release(&I.upd[p * nq + r], 1);
+      TRACE(kind, p, r);
+      continue;
     }
+    // X(p, r) = (A(p, r) - acc) Linv_r^T
+    if (tid == 0) s_ok = wait_ge(&I.flag[r * nq + r], 1, B.abort_flag) ? 1 : 0;
+    __syncthreads();
+    if (!s_ok) continue;
+    load_async<SG>(bufL, I.Linv + (size_t)r * T * T, T, T, T, tid);
+    cp_async_commit();
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int row = wm * 32 + mi * 16 + g + h * 8;
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int col = wn * 32 + ni * 8 + 2 * t + e;
+            double v = 0.0;
+            if (row < c.rows && col < c.cols) v = __ldcg(c.ptr + (size_t)row * ld + col) - acc[mi][ni][h * 2 + e];
+            bufA[row * SG + col] = v;
+          }
+      }
+    cp_async_wait<0>();
+    __syncthreads();
+    zero_acc(acc);
+    mma_nt(bufA, bufL, (c.cols + 3) & ~3, acc, wm, wn, g, t);
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int row = wm * 32 + mi * 16 + g + h * 8;
+        if (row >= c.rows) continue;
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int col = wn * 32 + ni * 8 + 2 * t + e;
+            if (col < c.cols) c.ptr[(size_t)row * ld + col] = acc[mi][ni][h * 2 + e];
+          }
+      }
+    release(&I.flag[p * nq + r], 1);
+    TRACE(kind, p, r);
   }
 }
 
@@ -317,6 +390,12 @@ extern "C" int bta_trace_setup(unsigned long long* buf) {
 }
 #endif
 
+// Queue order: one task per tile, column by column; within a column the two
+// tiles the chain CTA consumes next (the diagonal tile and the one below it)
+// come first, then the remaining rows of the diagonal block, then the rows of
+// the block below and of the arrow.  Every task only waits on outputs of
+// earlier columns or of the chain, so the order is topological.  Instances
+// are interleaved column by column.
 void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks) {
   int max_nq = 0;
   for (const auto& I : insts) max_nq = std::max(max_nq, I.nq);
@@ -324,16 +403,22 @@ void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks) 
     for (int ii = 0; ii < (int)insts.size(); ++ii) {
       const PanelInst& I = insts[ii];
       if (r >= I.nq) continue;
-      // updates of tile column r from every earlier column k (the chain CTA
-      // applies the last one to the diagonal tile itself)
-      for (int k = 0; k < r; ++k)
-        for (int p = r; p < I.nrows_t; ++p)
-          if (!(p == r && k == r - 1)) tasks.push_back(make_int4(ii, TASK_UPDATE, p, (r << 16) | k));
-      // TRSM below the diagonal, except the sub-diagonal tile the chain takes
-      for (int p = r + 1; p < I.nrows_t; ++p)
-        if (!(p == r + 1 && r + 1 < I.nq)) tasks.push_back(make_int4(ii, TASK_TRSM, p, (r << 16) | r));
+      tasks.push_back(make_int4(ii, TASK_AGG_DIAG, r, r));
+      if (r + 1 < I.nq) tasks.push_back(make_int4(ii, TASK_AGG_SUB, r + 1, r));
+    }
+    for (int ii = 0; ii < (int)insts.size(); ++ii) {
+      const PanelInst& I = insts[ii];
+      if (r >= I.nq) continue;
+      for (int p = r + 2; p < I.nq; ++p) tasks.push_back(make_int4(ii, TASK_AGG_TRSM, p, r));
+    }
+    for (int ii = 0; ii < (int)insts.size(); ++ii) {
+      const PanelInst& I = insts[ii];
+      if (r >= I.nq) continue;
+      for (int p = std::max(I.nq, r + 1); p < I.nrows_t; ++p) tasks.push_back(make_int4(ii, TASK_AGG_TRSM, p, r));
     }
   }
+  for (int ii = 0; ii < (int)insts.size(); ++ii)
+    if (insts[ii].Ttip != nullptr) tasks.push_back(make_int4(ii, TASK_TIP, 0, 0));
 }
 
 int panel_grid_size() {

@@ -2,16 +2,20 @@
 //
 // The panel of step i is the tall matrix [D_i; L_i; Ab_i] (tile rows of the
 // diagonal block, of the block below it, and of the arrow), cut into 64x64
-// tiles with nq = ceil(b/64) tile columns.  It is factored in place by
-//   POTRF(q)       D_i[q][q] <- chol(D_i[q][q]);  Linv_q <- its inverse
-//   TRSM(p, q)     tile(p, q) <- tile(p, q) * Linv_q^T           (p below q)
-//   UPDATE(p,r,q)  tile(p, r) <- tile(p, r) - tile(p, q) tile(r, q)^T
-// The critical path -- TRSM(q, q-1), UPDATE(q, q, q-1), POTRF(q) for
-// q = 0..nq-1 -- runs in one dedicated "chain" CTA per instance that keeps the
-// inverse of the previous diagonal tile in shared memory.  Every other task is
+// tiles with nq = ceil(b/64) tile columns, and factored in place:
+//   X(p, r) = (A(p, r) - sum_{k<r} X(p, k) X(r, k)^T) Linv_r^T   (p > r)
+//   L_rr    = chol(A(r, r) - sum_{k<r} X(r, k) X(r, k)^T),  Linv_r = L_rr^-1
+// When Lprev / Abprev are given, every tile task first applies the previous
+// block column's Schur update (D -= Lprev Lprev^T, Ab -= Abprev Lprev^T) and
+// a tip task applies T -= Ab Ab^T, so a whole BTA step is one launch.
+// The critical path -- X(q, q-1), the last update of tile (q, q), POTRF(q) and
+// Linv_q for q = 0..nq-1 -- runs in one dedicated "chain" CTA per instance that
+// keeps Linv_{q-1} in shared memory.  Every other tile is one left-looking task
 // claimed from a queue in a fixed topological order by the remaining
-// persistent CTAs.  Dependencies are tracked per tile with release/acquire
-// counters; every wait is bounded and sets an abort flag instead of hanging.
+// persistent CTAs: it accumulates its updates in registers as the source
+// columns become final, then applies its TRSM (or hands the tile to the
+// chain).  Dependencies are release/acquire flags per tile; every wait is
+// bounded and sets an abort flag instead of hanging.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -25,8 +29,12 @@ struct PanelInst {
   double* L;     // b x b block below D, or nullptr
   double* Ab;    // a x b arrow rows, or nullptr
   double* Linv;  // workspace: nq tiles of 64x64 (inverses of the diagonal tiles)
-  int* upd;      // [nrows_t * nq] number of column updates applied to a tile
-  int* flag;     // [nrows_t * nq] tile final (potrf / trsm done)
+  const double* Lprev;   // factor block below the previous diagonal block (its
+                         // rows are this D's rows), or nullptr
+  const double* Abprev;  // previous arrow block, or nullptr
+  double* Ttip;          // arrow tip (a x a, a <= 64) updated by this panel, or nullptr
+  int* upd;      // [nrows_t * nq] chain input tile accumulated (set to 1)
+  int* flag;     // [nrows_t * nq] tile final (X computed; diagonal: Linv ready)
   unsigned long long* info;  // min failing pivot (1-based global index)
   long long pivot_base;      // global row index of D's first row
   int b, a, nq, nrows_t;
@@ -37,13 +45,18 @@ constexpr int PANEL_MAXI = 64;
 struct PanelBatch {
   int ninst;
   int ntasks;
-  const int4* tasks;  // queue tasks {inst, kind, p, (r << 16) | q}
+  const int4* tasks;  // queue tasks {inst, kind, p, r}: one per tile (p, r)
   int* counter;       // [0] next queue task, [1] next chain role
   int* abort_flag;    // set on a timed-out wait (all later waits return)
   PanelInst inst[PANEL_MAXI];
 };
 
-enum : int { TASK_POTRF = 0, TASK_TRSM = 1, TASK_UPDATE = 2 };
+// Queue task kinds: the left-looking accumulation into a tile that the chain
+// CTA finishes (the diagonal tile, without its last update; the tile below
+// the diagonal), or accumulation followed by the TRSM with the inverse of the
+// column's diagonal tile.
+// TASK_TIP subtracts the panel's arrow rows from the tip: T -= X_a X_a^T.
+enum : int { TASK_AGG_DIAG = 3, TASK_AGG_SUB = 4, TASK_AGG_TRSM = 5, TASK_TIP = 6 };
 
 // Number of tile rows of a panel (diag rows, lower rows, arrow rows).
 inline int panel_rows(int b, int a, bool has_L) {
@@ -51,7 +64,7 @@ inline int panel_rows(int b, int a, bool has_L) {
   return nq + (has_L ? nq : 0) + (a + 63) / 64;
 }
 
-// Queue tasks (everything except the chain) of all instances, stage by stage.
+// Queue tasks (every tile except those the chain finishes) of all instances.
 void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks);
 
 // Launch one panel batch.  The counters of every instance, batch.counter[0..1]

@@ -103,7 +103,51 @@ __device__ __forceinline__ void gemv_t_sub(const double* M, int ld, int rows, in
   __syncthreads();
 }
 
+constexpr int SP = T + 1;  // smem stride of the prefetched tiles
+
+// Prefetch a rows x cols tile (ld) into smem (stride SP), zero-filled.
+__device__ __forceinline__ void prefetch_tile(double* s, const double* g, int ld, int rows, int cols, int tid) {
+#pragma unroll 4
+  for (int idx = tid; idx < T * T; idx += THREADS) {
+    const int r = idx >> 6, c = idx & 63;
+    s[r * SP + c] = (r < rows && c < cols) ? __ldg(g + (size_t)r * ld + c) : 0.0;
+  }
+}
+
+// acc[r] -= sum_c S[r][c] v[c] from smem (two threads per row)
+__device__ __forceinline__ void smem_gemv_sub(const double* S, const double* v, double* acc, int rows, int tid) {
+  const int r = tid >> 1, h = tid & 1;
+  double s = 0.0;
+#pragma unroll 8
+  for (int j = 0; j < 32; ++j) s += S[r * SP + h * 32 + j] * v[h * 32 + j];
+  s += __shfl_xor_sync(0xffffffffu, s, 1);
+  if (h == 0 && r < rows) acc[r] -= s;
+}
+
+// acc[c] -= sum_r S[r][c] v[r] from smem (two threads per column)
+__device__ __forceinline__ void smem_gemv_t_sub(const double* S, const double* v, double* acc, double* part,
+                                                int cols, int tid) {
+  const int c = tid & 63, h = tid >> 6;
+  double s = 0.0;
+#pragma unroll 8
+  for (int j = 0; j < 32; ++j) s += S[(h * 32 + j) * SP + c] * v[h * 32 + j];
+  part[tid] = s;
+  __syncthreads();
+  if (tid < cols) acc[tid] -= part[tid] + part[tid + 64];
+  __syncthreads();
+}
+
+// One sweep.  Task (i, p) owns tile row p of block i.  It prefetches the tile
+// that multiplies its last dependency (forward: the tile left of its diagonal
+// tile, or the last tile of the block below's row for p = 0; backward: the
+// transposed tile below its diagonal tile, or of the next block for the last
+// tile row) and the inverse of its diagonal tile, accumulates every other
+// contribution as its inputs are published, and only then waits for the last
+// one: the critical path per tile is two small GEMVs from shared memory.
 __global__ void __launch_bounds__(THREADS) sweep_kernel(SweepArgs A) {
+  extern __shared__ __align__(16) double sm[];
+  double* Sc = sm;           // critical tile
+  double* Sl = sm + T * SP;  // inverse of the diagonal tile
   __shared__ double acc[T], v[T], part[2 * T];
   __shared__ int s_task, s_ok;
   const int tid = threadIdx.x;
@@ -124,14 +168,52 @@ __global__ void __launch_bounds__(THREADS) sweep_kernel(SweepArgs A) {
     }
     const int rows = min(T, A.b - p * T);
     double* xi = A.x + (size_t)i * A.b;
+    // --- prefetch the critical tile and the diagonal-tile inverse
+    const double* crit = nullptr;
+    int crows = 0, ccols = 0, cflag = -1;
+    const double* cvec = nullptr;
+    if (A.trans == 0) {
+      if (p > 0) {
+        crit = A.D + (size_t)i * bb + (size_t)(p * T) * A.b + (p - 1) * T;
+        crows = rows;
+        ccols = T;
+        cflag = i * A.nq + p - 1;
+        cvec = xi + (p - 1) * T;
+      } else if (i > 0) {
+        const int kq = A.nq - 1;
+        crit = A.L + (size_t)(i - 1) * bb + kq * T;  // row tile 0, column tile nq-1
+        crows = rows;
+        ccols = min(T, A.b - kq * T);
+        cflag = (i - 1) * A.nq + kq;
+        cvec = A.x + (size_t)(i - 1) * A.b + kq * T;
+      }
+    } else {
+      if (p < A.nq - 1) {
+        crit = A.D + (size_t)i * bb + (size_t)((p + 1) * T) * A.b + p * T;  // tile (p+1, p)
+        crows = min(T, A.b - (p + 1) * T);
+        ccols = rows;
+        cflag = i * A.nq + p + 1;
+        cvec = xi + (p + 1) * T;
+      } else if (i < A.n - 1) {
+        crit = A.L + (size_t)i * bb + p * T;  // tile (0, p) of L_i
+        crows = min(T, A.b);
+        ccols = rows;
+        cflag = (i + 1) * A.nq;
+        cvec = A.x + (size_t)(i + 1) * A.b;
+      }
+    }
+    if (crit) prefetch_tile(Sc, crit, A.b, crows, ccols, tid);
+    prefetch_tile(Sl, A.Linv + (size_t)(i * A.nq + p) * T * T, T, rows, rows, tid);
     if (tid < T) acc[tid] = (tid < rows) ? xi[p * T + tid] : 0.0;
     __syncthreads();
     bool ok = true;
+    // --- every non-critical contribution
     if (A.trans == 0) {
       if (i > 0) {
         const double* Lm = A.L + (size_t)(i - 1) * bb + (size_t)(p * T) * A.b;
         const double* yprev = A.x + (size_t)(i - 1) * A.b;
-        for (int k = 0; k < A.nq && ok; ++k) {
+        const int klast = (p == 0) ? A.nq - 1 : A.nq;
+        for (int k = 0; k < klast && ok; ++k) {
           if (tid == 0) s_ok = wait_flag(&A.flags[(i - 1) * A.nq + k], A.abort_flag);
           __syncthreads();
           ok = s_ok;
@@ -145,7 +227,7 @@ __global__ void __launch_bounds__(THREADS) sweep_kernel(SweepArgs A) {
         }
       }
       const double* Dm = A.D + (size_t)i * bb + (size_t)(p * T) * A.b;
-      for (int k = 0; k < p && ok; ++k) {
+      for (int k = 0; k + 1 < p && ok; ++k) {
         if (tid == 0) s_ok = wait_flag(&A.flags[i * A.nq + k], A.abort_flag);
         __syncthreads();
         ok = s_ok;
@@ -156,34 +238,20 @@ __global__ void __launch_bounds__(THREADS) sweep_kernel(SweepArgs A) {
         }
         __syncthreads();
       }
-      if (ok) {
-        // y = Linv_pp * acc
-        const double* Li = A.Linv + (size_t)(i * A.nq + p) * T * T;
-        if (tid < T) v[tid] = acc[tid];
-        if (tid < T) acc[tid] = 0.0;
-        __syncthreads();
-        gemv_sub(Li, T, rows, rows, v, acc, tid);
-        __syncthreads();
-        if (tid < rows) xi[p * T + tid] = -acc[tid];
-      }
     } else {
       if (A.a > 0) {
-        // acc -= Ab_i[:, p-tile]^T x_a
-        if (tid < T) v[tid] = tid < A.a ? __ldcg(A.x + (size_t)A.n * A.b + tid) : 0.0;
-        __syncthreads();
         for (int a0 = 0; a0 < A.a; a0 += T) {
           const int ar = min(T, A.a - a0);
-          if (a0 > 0) {
-            if (tid < T) v[tid] = tid < ar ? __ldcg(A.x + (size_t)A.n * A.b + a0 + tid) : 0.0;
-            __syncthreads();
-          }
+          if (tid < T) v[tid] = tid < ar ? __ldcg(A.x + (size_t)A.n * A.b + a0 + tid) : 0.0;
+          __syncthreads();
           gemv_t_sub(A.Ab + (size_t)i * A.a * A.b + (size_t)a0 * A.b + p * T, A.b, ar, rows, v, acc, part, tid);
         }
       }
       if (i < A.n - 1) {
         const double* Lm = A.L + (size_t)i * bb + p * T;
         const double* xnext = A.x + (size_t)(i + 1) * A.b;
-        for (int k = 0; k < A.nq && ok; ++k) {
+        const int kfirst = (p == A.nq - 1) ? 1 : 0;
+        for (int k = A.nq - 1; k >= kfirst && ok; --k) {
           if (tid == 0) s_ok = wait_flag(&A.flags[(i + 1) * A.nq + k], A.abort_flag);
           __syncthreads();
           ok = s_ok;
@@ -196,7 +264,7 @@ __global__ void __launch_bounds__(THREADS) sweep_kernel(SweepArgs A) {
         }
       }
       const double* Dm = A.D + (size_t)i * bb + p * T;
-      for (int k = A.nq - 1; k > p && ok; --k) {
+      for (int k = A.nq - 1; k > p + 1 && ok; --k) {
         if (tid == 0) s_ok = wait_flag(&A.flags[i * A.nq + k], A.abort_flag);
         __syncthreads();
         ok = s_ok;
@@ -207,15 +275,29 @@ __global__ void __launch_bounds__(THREADS) sweep_kernel(SweepArgs A) {
           gemv_t_sub(Dm + (size_t)(k * T) * A.b, A.b, kr, rows, v, acc, part, tid);
         }
       }
+    }
+    // --- the critical dependency, then the diagonal tile
+    if (ok && crit) {
+      if (tid == 0) s_ok = wait_flag(&A.flags[cflag], A.abort_flag);
+      __syncthreads();
+      ok = s_ok;
       if (ok) {
-        // x = Linv_pp^T * acc
-        const double* Li = A.Linv + (size_t)(i * A.nq + p) * T * T;
-        if (tid < T) v[tid] = acc[tid];
-        if (tid < T) acc[tid] = 0.0;
+        const int vn = (A.trans == 0) ? ccols : crows;
+        if (tid < T) v[tid] = tid < vn ? __ldcg(cvec + tid) : 0.0;
         __syncthreads();
-        gemv_t_sub(Li, T, rows, rows, v, acc, part, tid);
-        if (tid < rows) xi[p * T + tid] = -acc[tid];
+        if (A.trans == 0) smem_gemv_sub(Sc, v, acc, rows, tid);
+        else smem_gemv_t_sub(Sc, v, acc, part, rows, tid);
       }
+      __syncthreads();
+    }
+    if (ok) {
+      if (tid < T) v[tid] = acc[tid];
+      if (tid < T) acc[tid] = 0.0;
+      __syncthreads();
+      if (A.trans == 0) smem_gemv_sub(Sl, v, acc, rows, tid);
+      else smem_gemv_t_sub(Sl, v, acc, part, rows, tid);
+      __syncthreads();
+      if (tid < rows) xi[p * T + tid] = -acc[tid];
     }
     __syncthreads();
     if (tid == 0 && ok) {
@@ -294,10 +376,15 @@ int sweep_launch(const SweepArgs& A, cudaStream_t s) {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = std::min(total, sms * 8);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * T * SP * sizeof(double)));
+    attr = true;
+  }
+  const int grid = std::min(total, sms * 3);
   {
     bta::ProfScope _ps(bta::PROF_SWEEP, s);
-    sweep_kernel<<<grid, THREADS, 0, s>>>(A);
+    sweep_kernel<<<grid, THREADS, 2 * T * SP * sizeof(double), s>>>(A);
   }
   return cudaGetLastError();
 }

@@ -300,6 +300,31 @@ class SpatioTemporalModel:
         D, L, Ab, T = M.ptrs()
         self._check(self.lib.bta_pobtaf(self.h.bind_stream(), M.n, M.b, M.a, D, L, Ab, T, None), "pobtaf")
 
+    def _batched_args(self, mats):
+        k = len(mats)
+        i64 = ctypes.c_int64 * k
+        ptrs = ctypes.c_void_p * k
+        n = i64(*[m.n for m in mats])
+        b = i64(*[m.b for m in mats])
+        a = i64(*[m.a for m in mats])
+        P = [m.ptrs() for m in mats]
+        D = ptrs(*[p[0].value for p in P])
+        L = ptrs(*[p[1].value for p in P])
+        Ab = ptrs(*[p[2].value for p in P])
+        T = ptrs(*[p[3].value for p in P])
+        return k, n, b, a, D, L, Ab, T
+
+    def factor_batched(self, mats):
+        """All matrices factored together, block column by block column."""
+        k, n, b, a, D, L, Ab, T = self._batched_args(mats)
+        self._check(self.lib.bta_pobtaf_batched(self.h.bind_stream(), k, n, b, a, D, L, Ab, T, None),
+                    "pobtaf_batched")
+
+    def selinv_batched(self, mats):
+        k, n, b, a, D, L, Ab, T = self._batched_args(mats)
+        self._check(self.lib.bta_pobtasi_batched(self.h.bind_stream(), k, n, b, a, D, L, Ab, T),
+                    "pobtasi_batched")
+
     def logdet_to(self, M: BTAMatrix, slot):
         D, _, _, T = M.ptrs()
         out = _lib.ptr(self.scal[slot:slot + 1])
@@ -403,16 +428,15 @@ class SpatioTemporalModel:
         stream = self._stream()
         _lib.check(self.lib.bta_reset_status(self.h.bind_stream()), "reset")
         self.assemble_conditional(theta, None, tau)
-        self.factor(self.Qc)
+        self.assemble_prior_bt(theta)
+        self.factor_batched([self.Qc, self.Qp])
         self.logdet_to(self.Qc, 0)
+        self.logdet_to(self.Qp, 2)
         self._check(self.lib.bta_axpby(stream, self.N, tau, _lib.ptr(self.Aty), 0.0, _lib.ptr(self.rhs)), "axpby")
         self.x.copy_(self.rhs)
         self.sweep(self.Qc, self.x, 0)
         self.dot_to(self.x, self.x, 1)  # b^T Q^-1 b = |L^-1 b|^2
         self.sweep(self.Qc, self.x, 1)  # mu
-        self.assemble_prior_bt(theta)
-        self.factor(self.Qp)
-        self.logdet_to(self.Qp, 2)
         # |A mu|^2 and mu^T (E_tt' (x) K) mu
         self.spmv(self.A_rowptr, self.A_col, self.A_val, self.nobs, self.x, self.eta)
         self.dot_to(self.eta, self.eta, 3)
@@ -420,8 +444,7 @@ class SpatioTemporalModel:
                                             _lib.ptr(self.u_vals4), _lib.ptr(self.x), _lib.ptr(self.quad_st)),
                     "block_quad")
         # selected inverses and their contractions
-        self.selinv(self.Qc)
-        self.selinv(self.Qp)
+        self.selinv_batched([self.Qc, self.Qp])
         Dc, Lc, _, _ = self.Qc.ptrs()
         Dp, Lp, _, _ = self.Qp.ptrs()
         for (Dm, Lm, out) in ((Dc, Lc, self.inner_c), (Dp, Lp, self.inner_p)):

@@ -58,6 +58,21 @@ int bta_pobtaf(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, doubl
                int64_t* info);
 
 /*
+ * Batched forms: count independent BTA matrices (instance k has sizes n[k],
+ * b[k], a[k] and arrays D[k], L[k], Ab[k], T[k]; L/Ab/T entries may be NULL
+ * where unused) factored / selected-inverted together, block column by block
+ * column, so that the critical paths of all instances run concurrently in one
+ * launch.  This is the batched launch over the theta points of a
+ * finite-difference stencil or a line search (the reference evaluates them one
+ * after another, src/dalia/core/dalia.py:558-564).  For the batched
+ * factorisation, info = k * 2^40 + pivot identifies instance k.
+ */
+int bta_pobtaf_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                       double* const* D, double* const* L, double* const* Ab, double* const* T, int64_t* info);
+int bta_pobtasi_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                        double* const* D, double* const* L, double* const* Ab, double* const* T);
+
+/*
  * One triangular sweep with the factor, in place on rhs (length n*b + a).
  * trans = 0: solve L y = rhs (Serinv trans="N"); trans = 1: solve L^T x = rhs
  * (trans="C").  Replaces pobtas (structured_solver.py:112-127) and, with a = 0,

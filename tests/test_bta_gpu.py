@@ -121,3 +121,43 @@ def test_not_positive_definite_raises():
     D2, L2, Ab2, T2 = bta_ref.random_bta(2, 30, 1, rng)
     d2 = _cuda(D2, L2, Ab2, T2)
     sc.pobtaf(*d2)
+
+
+def test_batched_factor_and_selinv_match_single():
+    """Instances of different sizes in one batched launch give the results of
+    separate calls."""
+    import ctypes
+
+    import torch
+
+    from dalia_b200 import _lib
+
+    lib = _lib.load()
+    h = _lib.handle()
+    shapes = [(4, 130, 3), (3, 64, 0), (5, 70, 6), (2, 200, 1)]
+    rng = np.random.default_rng(11)
+    mats = [bta_ref.random_bta(n, b, a, rng) for n, b, a in shapes]
+    single = [_cuda(*m) for m in mats]
+    batch = [_cuda(*m) for m in mats]
+    for (n, b, a), t in zip(shapes, single):
+        assert lib.bta_pobtaf(h.bind_stream(), n, b, a, *[_lib.ptr(x if x.numel() else None) for x in t], None) == 0
+    k = len(shapes)
+    I64, P = ctypes.c_int64 * k, ctypes.c_void_p * k
+    args = (I64(*[s[0] for s in shapes]), I64(*[s[1] for s in shapes]), I64(*[s[2] for s in shapes]),
+            *[P(*[(t[j].data_ptr() if t[j].numel() else None) for t in batch]) for j in range(4)])
+    info = ctypes.c_int64(-1)
+    assert lib.bta_pobtaf_batched(h.bind_stream(), k, *args, ctypes.byref(info)) == 0 and info.value == 0
+    for s_, b_ in zip(single, batch):
+        for x, y in zip(s_, b_):
+            if x.numel():
+                assert rel(y.cpu().numpy(), x.cpu().numpy()) < TOL
+    for (n, b, a), t in zip(shapes, single):
+        assert lib.bta_pobtasi(h.bind_stream(), n, b, a, *[_lib.ptr(x if x.numel() else None) for x in t]) == 0
+    assert lib.bta_pobtasi_batched(h.bind_stream(), k, *args) == 0
+    torch.cuda.synchronize()
+    for (n, b, a), m, s_, b_ in zip(shapes, mats, single, batch):
+        S = bta_ref.dense_to_bta(np.linalg.inv(bta_ref.bta_to_dense(*m)), n, b, a)
+        for j, (x, y) in enumerate(zip(s_, b_)):
+            if x.numel():
+                assert rel(y.cpu().numpy(), x.cpu().numpy()) < TOL
+                assert rel(y.cpu().numpy(), S[j]) < TOL
