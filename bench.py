@@ -4,10 +4,13 @@ nt = 100, nb = 6, 600 observations per step; BTA blocks 1500 x 1500).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One step = one full gradient evaluation (f(theta) and grad f) at the
-workload's theta.  ``ours`` uses the adjoint path (one factorisation and
-selected inversion of Q_c and of Q_prior); the plain FP64 central-difference
-path (2d+1 evaluations of f, as the reference computes it) is timed beside it.
+One step = full gradient evaluations (f(theta) and grad f) at ``--batch``
+theta points (the candidates of a line search, default 3), the unit counted
+being one gradient evaluation.  ``ours`` uses the adjoint path (one
+factorisation and selected inversion of Q_c and of Q_prior per point, all 2K
+matrices factored and inverted together); the single-point adjoint and the
+plain FP64 central-difference path (2d+1 evaluations of f, one after another,
+as the reference computes it) are timed beside it.
 With N > 1 (torchrun) every rank evaluates its own replica (independent theta
 points, no collective on the data path); the reported value is the total over
 ranks divided by the slowest rank's device time.
@@ -47,6 +50,9 @@ def parse():
     p.add_argument("--workload", default="gst_1500x100")
     p.add_argument("--cpu-nt", type=int, default=10)
     p.add_argument("--fd-steps", type=int, default=1)
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU-oracle baseline sample")
+    p.add_argument("--batch", type=int, default=3,
+                   help="theta points per step (a line-search batch), factorised together")
     return p.parse_args()
 
 
@@ -181,18 +187,13 @@ def measured_fp64_peak(torch, dev):
     return 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
-def panel_flops(n, b, a):
-    """Algorithmic flops of the panel kernels of one BTA factorisation:
-    per block column POTRF b^3/3, TRSM of the block below b^3, arrow a b^2;
-    plus the tip a^3/3."""
-    f = n * (b ** 3 / 3 + a * b ** 2) + (n - 1) * b ** 3
+def factor_flops(n, b, a):
+    """Algorithmic flops of one BTA factorisation, all done by the panel
+    kernel (one launch per block column): POTRF b^3/3, TRSM of the block below
+    b^3 and of the arrow a b^2, the previous column's Schur update b^3 (SYRK,
+    lower half), 2ab^2 (arrow) and a^2 b (tip); plus the tip POTRF a^3/3."""
+    f = n * (b ** 3 / 3 + a * b ** 2 + a * a * b) + (n - 1) * (b ** 3 + b ** 3 + 2 * a * b ** 2)
     return f + a ** 3 / 3
-
-
-def gemm_flops_factor(n, b, a):
-    """Trailing updates of one factorisation: SYRK b^3 (lower half of 2b^3),
-    arrow 2ab^2 and tip a^2 b per block column."""
-    return (n - 1) * (b ** 3 + 2 * a * b ** 2) + n * (a * a * b)
 
 
 def gemm_flops_selinv(n, b, a):
@@ -229,12 +230,15 @@ def run_ours(args):
         if world > 1:
             torch.distributed.barrier()
 
+    K = max(1, args.batch)
+    thetas = [theta + 1e-3 * j for j in range(K)]
+
     # ---- warm-up
     for _ in range(max(args.warmup, 3)):
-        model.objective_adjoint(theta)
+        model.objective_adjoint_batched(thetas)
     barrier()
 
-    # ---- device-timed adjoint steps (roofline events on)
+    # ---- device-timed steps: K-point adjoint gradient batches (roofline events on)
     clock = ClockSampler(local)
     clock.start()
     lib.bta_prof_read(None, None)
@@ -244,7 +248,7 @@ def run_ours(args):
     e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
     e0.record()
     for _ in range(args.steps):
-        model.objective_adjoint(theta)
+        model.objective_adjoint_batched(thetas)
     e1.record()
     barrier()
     launches = lib.bta_launch_count() - launches0
@@ -258,42 +262,53 @@ def run_ours(args):
         tt = torch.tensor([t_dev], device=dev)
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
         t_dev = float(tt.item())
-    value = args.steps * world / t_dev
+    value = K * args.steps * world / t_dev
 
-    # ---- end to end through the public call, host theta in, host gradient out
+    # ---- single-point adjoint latency
+    barrier()
+    s0, s1 = torch.cuda.Event(True), torch.cuda.Event(True)
+    s0.record()
+    for _ in range(args.steps):
+        model.objective_adjoint(theta)
+    s1.record()
+    barrier()
+    single_rate = args.steps / (s0.elapsed_time(s1) * 1e-3)
+
+    # ---- end to end through the public call, host thetas in, host gradients out
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        th_host = np.array(theta)  # host buffer
-        f, g = model.objective_adjoint(th_host)
+        th_host = [np.array(t) for t in thetas]  # host buffers
+        fs, gs = model.objective_adjoint_batched(th_host)
     torch.cuda.synchronize()
     t_e2e = time.perf_counter() - t0
     if world > 1:
         tt = torch.tensor([t_e2e], device=dev)
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
         t_e2e = float(tt.item())
-    e2e = args.steps * world / t_e2e
-    coef_bytes = model.coef_host.numel() * 8
-    h2d = 2 * coef_bytes
-    d2h = (5 + 3 * (2 * n - 1) * 4 + a * a) * 8 + 16
+    e2e = K * args.steps * world / t_e2e
+    f, g = fs[0], gs[0]
+    coef_bytes = model.slots[0].coef_host[0].numel() * 8
+    h2d = K * 2 * coef_bytes
+    d2h = K * ((5 + 3 * (2 * n - 1) * 4 + a * a) * 8) + 16
 
     # ---- plain FP64 finite differences (the reference's algorithm)
-    barrier()
-    f0, f1 = torch.cuda.Event(True), torch.cuda.Event(True)
-    f0.record()
-    for _ in range(args.fd_steps):
-        model.objective_fd(theta)
-    f1.record()
-    barrier()
-    t_fd = f0.elapsed_time(f1) * 1e-3
-    fd_rate = args.fd_steps / t_fd
+    fd_rate = None
+    if args.fd_steps > 0:
+        barrier()
+        f0, f1 = torch.cuda.Event(True), torch.cuda.Event(True)
+        f0.record()
+        for _ in range(args.fd_steps):
+            model.objective_fd(theta)
+        f1.record()
+        barrier()
+        fd_rate = args.fd_steps / (f0.elapsed_time(f1) * 1e-3)
 
     # ---- roofline of the dominant kernel category
     names = {0: "panel (tile-DAG BTA panel Cholesky)", 1: "gemm (grouped FP64 DMMA GEMM)"}
     per_step_flops = {
-        0: panel_flops(n, b, a) + panel_flops(n, b, 0),
-        1: gemm_flops_factor(n, b, a) + gemm_flops_factor(n, b, 0) + gemm_flops_selinv(n, b, a)
-        + gemm_flops_selinv(n, b, 0),
+        0: K * (factor_flops(n, b, a) + factor_flops(n, b, 0)),
+        1: K * (gemm_flops_selinv(n, b, a) + gemm_flops_selinv(n, b, 0)),
     }
     dom = max((0, 1), key=lambda c: ms_cat[c])
     achieved = per_step_flops[dom] * args.steps / (ms_cat[dom] * 1e-3) / 1e12
@@ -319,7 +334,7 @@ def run_ours(args):
     kernel_ms = {k: ms_cat[i] / args.steps for i, k in enumerate(["panel", "gemm", "sweep", "trtri", "other"])}
 
     cpu = None
-    if rank == 0:
+    if rank == 0 and not args.no_cpu:
         try:
             t_cpu, desc = cpu_sample(args.workload, args.cpu_nt)
             cpu = {"value": 1.0 / t_cpu, "unit": "evals/s", "cores": os.cpu_count(), "kind": "port", "sample": desc}
@@ -327,7 +342,6 @@ def run_ours(args):
             cpu = {"value": None, "unit": "evals/s", "cores": os.cpu_count(), "kind": "port", "sample": repr(exc)}
 
     if rank == 0:
-        f_fac = 2 * (panel_flops(n, b, a) + gemm_flops_factor(n, b, a))
         line = {
             "metric": METRIC,
             "value": value,
@@ -344,7 +358,9 @@ def run_ours(args):
             "config": {
                 "workload": args.workload,
                 "ns": b, "nt": n, "nb": a, "obs_per_step": cfg["no"], "theta": list(cfg["theta"]),
-                "path": "adjoint gradient, FP64 (factor + selected inversion of Q_c and Q_prior)",
+                "path": f"adjoint gradient, FP64; {K} theta points per step (line-search batch): "
+                        f"{2 * K} BTA factorisations + selected inversions per launch sequence",
+                "theta_points_per_step": K,
                 "parallelism": f"replicas x{world}",
                 "l2": "inputs larger than L2 (BTA factor 3.6 GB per matrix)",
             },
@@ -354,7 +370,10 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "clocks": clocks,
             "fd_fp64_evals_per_s": fd_rate,
-            "speedup_vs_fd_fp64": value / fd_rate,
+            "adjoint_single_point_evals_per_s": single_rate,
+            "speedup_vs_fd_fp64": (value / fd_rate) if fd_rate else None,
+            "bta_factor_tflops": per_step_flops[0] * args.steps / (ms_cat[0] * 1e-3) / 1e12,
+            "bta_selinv_gemm_tflops": per_step_flops[1] * args.steps / (ms_cat[1] * 1e-3) / 1e12,
             "kernel_ms_per_step": kernel_ms,
             "f": f,
             "grad": list(map(float, g)),

@@ -334,42 +334,63 @@ int bta_pobtaf(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, doubl
   return bta_pobtaf_batched(h, 1, &n, &b, &a, &D, &L, &Ab, &T, info);
 }
 
-int bta_pobtas(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D, const double* L,
-               const double* Ab, const double* T, double* rhs, int trans) {
-  if (!h || n < 1 || b < 1 || a < 0 || !D || !rhs || (n > 1 && !L) || (a > 0 && (!Ab || !T))) return BTA_ERR_INVALID;
+int bta_pobtas_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                       const double* const* D, const double* const* L, const double* const* Ab,
+                       const double* const* T, double* const* rhs, int trans) {
+  if (!h || count < 1 || count > SWEEP_MAXI || !n || !b || !a || !D || !rhs) return BTA_ERR_INVALID;
   if (trans != 0 && trans != 1) return BTA_ERR_INVALID;
-  const int nq = (int)((b + 63) / 64);
-  const size_t need = align_up((size_t)n * nq * 4096 * 8) + align_up(((size_t)n * nq + 4) * 4) + kAlign;
+  size_t need = 4 * kAlign;
+  for (int k = 0; k < count; ++k) {
+    if (n[k] < 1 || b[k] < 1 || a[k] < 0 || !D[k] || !rhs[k] || (n[k] > 1 && (!L || !L[k])) ||
+        (a[k] > 0 && (!Ab || !T || !Ab[k] || !T[k])))
+      return BTA_ERR_INVALID;
+    const size_t nq = (b[k] + 63) / 64;
+    need += align_up(n[k] * nq * 4096 * 8) + align_up((n[k] * nq + 4) * 4) + 2 * kAlign;
+  }
   int rc = ensure_ws(h, need);
   if (rc) return rc;
   cudaStream_t s = h->stream;
   Carve cv{h->ws};
-  double* tinv = cv.take<double>((size_t)n * nq * 4096);
-  int* flags = cv.take<int>((size_t)n * nq + 4);
-  if (cudaMemsetAsync(flags, 0, ((size_t)n * nq + 4) * sizeof(int), s) != cudaSuccess) return BTA_ERR_CUDA;
-  if (diag_tile_inverses(D, (int)n, (int)b, tinv, s)) return BTA_ERR_CUDA;
-  SweepArgs A{};
-  A.D = D;
-  A.L = L;
-  A.Ab = Ab;
-  A.Linv = tinv;
-  A.x = rhs;
-  A.flags = flags;
-  A.counter = flags + n * nq;
-  A.abort_flag = h->ctl;
-  A.n = (int)n;
-  A.b = (int)b;
-  A.a = (int)a;
-  A.nq = nq;
-  A.trans = trans;
-  if (trans == 0) {
-    if (sweep_launch(A, s)) return BTA_ERR_CUDA;
-    if (arrow_forward(Ab, T, rhs, (int)n, (int)b, (int)a, s)) return BTA_ERR_CUDA;
-  } else {
-    if (arrow_backward(T, rhs, (int)n, (int)b, (int)a, s)) return BTA_ERR_CUDA;
-    if (sweep_launch(A, s)) return BTA_ERR_CUDA;
+  int* counter = cv.take<int>(4);
+  if (cudaMemsetAsync(counter, 0, 4 * sizeof(int), s) != cudaSuccess) return BTA_ERR_CUDA;
+  SweepBatch B;
+  std::memset(&B, 0, sizeof(B));
+  B.count = count;
+  B.counter = counter;
+  for (int k = 0; k < count; ++k) {
+    const int nq = (int)((b[k] + 63) / 64);
+    double* tinv = cv.take<double>((size_t)n[k] * nq * 4096);
+    int* flags = cv.take<int>((size_t)n[k] * nq + 4);
+    if (cudaMemsetAsync(flags, 0, ((size_t)n[k] * nq + 4) * sizeof(int), s) != cudaSuccess) return BTA_ERR_CUDA;
+    if (diag_tile_inverses(D[k], (int)n[k], (int)b[k], tinv, s)) return BTA_ERR_CUDA;
+    SweepArgs& A = B.inst[k];
+    A.D = D[k];
+    A.L = L ? L[k] : nullptr;
+    A.Ab = Ab ? Ab[k] : nullptr;
+    A.Linv = tinv;
+    A.x = rhs[k];
+    A.flags = flags;
+    A.counter = counter;
+    A.abort_flag = h->ctl;
+    A.n = (int)n[k];
+    A.b = (int)b[k];
+    A.a = (int)a[k];
+    A.nq = nq;
+    A.trans = trans;
+    if (trans == 1 && arrow_backward(T[k], rhs[k], (int)n[k], (int)b[k], (int)a[k], s)) return BTA_ERR_CUDA;
   }
+  if (sweep_launch_batched(B, s)) return BTA_ERR_CUDA;
+  if (trans == 0)
+    for (int k = 0; k < count; ++k)
+      if (arrow_forward(Ab ? Ab[k] : nullptr, T ? T[k] : nullptr, rhs[k], (int)n[k], (int)b[k], (int)a[k], s))
+        return BTA_ERR_CUDA;
   return cuda_rc(cudaGetLastError());
+}
+
+int bta_pobtas(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D, const double* L,
+               const double* Ab, const double* T, double* rhs, int trans) {
+  if (!h || n < 1 || b < 1 || a < 0 || !D || !rhs || (n > 1 && !L) || (a > 0 && (!Ab || !T))) return BTA_ERR_INVALID;
+  return bta_pobtas_batched(h, 1, &n, &b, &a, &D, &L, &Ab, &T, &rhs, trans);
 }
 
 int bta_pobtasi_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,

@@ -19,8 +19,20 @@ struct SweepArgs {
   int trans;  // 0: L y = x,  1: L^T x = y
 };
 
+constexpr int SWEEP_MAXI = 32;
+
+// Several independent sweeps in one launch; tasks of the instances interleave
+// (task t belongs to instance t % count), each instance keeps its own order.
+struct SweepBatch {
+  int count;
+  int total;  // count * max_tasks
+  int* counter;
+  SweepArgs inst[SWEEP_MAXI];
+};
+
 int diag_tile_inverses(const double* D, int n, int b, double* out, cudaStream_t s);
 int sweep_launch(const SweepArgs& A, cudaStream_t s);
+int sweep_launch_batched(SweepBatch& B, cudaStream_t s);
 int arrow_forward(const double* Ab, const double* T, double* x, int n, int b, int a, cudaStream_t s);
 int arrow_backward(const double* T, double* x, int n, int b, int a, cudaStream_t s);
 

@@ -6,6 +6,7 @@
 // it depends on are published (release/acquire flags, bounded waits) and then
 // applies the inverse of its diagonal tile.
 #include <algorithm>
+#include <cstring>
 
 #include "bta_internal.cuh"
 #include "common.cuh"
@@ -144,20 +145,22 @@ __device__ __forceinline__ void smem_gemv_t_sub(const double* S, const double* v
 // tile row) and the inverse of its diagonal tile, accumulates every other
 // contribution as its inputs are published, and only then waits for the last
 // one: the critical path per tile is two small GEMVs from shared memory.
-__global__ void __launch_bounds__(THREADS) sweep_kernel(SweepArgs A) {
+__global__ void __launch_bounds__(THREADS) sweep_kernel(const __grid_constant__ SweepBatch BT) {
   extern __shared__ __align__(16) double sm[];
   double* Sc = sm;           // critical tile
   double* Sl = sm + T * SP;  // inverse of the diagonal tile
   __shared__ double acc[T], v[T], part[2 * T];
   __shared__ int s_task, s_ok;
   const int tid = threadIdx.x;
-  const int total = A.n * A.nq;
-  const size_t bb = (size_t)A.b * A.b;
   for (;;) {
-    if (tid == 0) s_task = atomicAdd(A.counter, 1);
+    if (tid == 0) s_task = atomicAdd(BT.counter, 1);
     __syncthreads();
-    const int ti = s_task;
-    if (ti >= total) break;
+    const int tb = s_task;
+    if (tb >= BT.total) break;
+    const SweepArgs& A = BT.inst[tb % BT.count];
+    const int ti = tb / BT.count;
+    if (ti >= A.n * A.nq) continue;
+    const size_t bb = (size_t)A.b * A.b;
     int i, p;
     if (A.trans == 0) {
       i = ti / A.nq;
@@ -370,9 +373,11 @@ int diag_tile_inverses(const double* D, int n, int b, double* out, cudaStream_t 
   return cudaGetLastError();
 }
 
-int sweep_launch(const SweepArgs& A, cudaStream_t s) {
-  const int total = A.n * A.nq;
-  if (total == 0) return cudaSuccess;
+int sweep_launch_batched(SweepBatch& B, cudaStream_t s) {
+  int maxt = 0;
+  for (int k = 0; k < B.count; ++k) maxt = std::max(maxt, B.inst[k].n * B.inst[k].nq);
+  B.total = B.count * maxt;
+  if (B.total == 0) return cudaSuccess;
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -381,12 +386,21 @@ int sweep_launch(const SweepArgs& A, cudaStream_t s) {
     cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * T * SP * sizeof(double)));
     attr = true;
   }
-  const int grid = std::min(total, sms * 3);
+  const int grid = std::min(B.total, sms * 3);
   {
     bta::ProfScope _ps(bta::PROF_SWEEP, s);
-    sweep_kernel<<<grid, THREADS, 2 * T * SP * sizeof(double), s>>>(A);
+    sweep_kernel<<<grid, THREADS, 2 * T * SP * sizeof(double), s>>>(B);
   }
   return cudaGetLastError();
+}
+
+int sweep_launch(const SweepArgs& A, cudaStream_t s) {
+  SweepBatch B;
+  std::memset(&B, 0, sizeof(B));
+  B.count = 1;
+  B.counter = A.counter;
+  B.inst[0] = A;
+  return sweep_launch_batched(B, s);
 }
 
 int arrow_forward(const double* Ab, const double* Tt, double* x, int n, int b, int a, cudaStream_t s) {

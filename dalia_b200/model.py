@@ -120,6 +120,29 @@ class BTAMatrix:
         return P(self.D), P(L), P(None), P(None)
 
 
+class _Slot:
+    """Device state of one theta point: the two BTA matrices, vectors and
+    read-back scalars (one per point of a batched evaluation)."""
+
+    def __init__(self, n, b, a, N, nobs, device, Qc=None, Qp=None):
+        import torch
+
+        f64 = dict(dtype=torch.float64, device=device)
+        self.Qc = Qc if Qc is not None else BTAMatrix(n, b, a, device)
+        self.Qp = Qp if Qp is not None else BTAMatrix(n, b, 0, device)
+        self.rhs = torch.zeros(N, **f64)
+        self.x = torch.zeros(N, **f64)  # latent mean / mode, like the reference's model.x
+        self.eta = torch.zeros(nobs, **f64)
+        self.scal = torch.zeros(16, **f64)
+        nb4 = (2 * n - 1) * 4
+        self.inner_c = torch.zeros(nb4, **f64)
+        self.inner_p = torch.zeros(nb4, **f64)
+        self.quad_st = torch.zeros(nb4, **f64)
+        # one pinned host buffer per assembly so that queued copies never race
+        self.coef_host = [torch.zeros(nb4, dtype=torch.float64).pin_memory() for _ in range(2)]
+        self.coef_dev = [torch.zeros(nb4, **f64) for _ in range(2)]
+
+
 class SpatioTemporalModel:
     """DEMF(1,2,1) spatio-temporal field + fixed effects, Gaussian or Poisson
     likelihood, evaluated on one GPU."""
@@ -185,6 +208,7 @@ class SpatioTemporalModel:
         # --- A^T D A entry lists on the BTA pattern (tip handled separately)
         self.Qc = BTAMatrix(n, b, a, dev)
         self.Qp = BTAMatrix(n, b, 0, dev)
+        self._dev = dev
         first, second, row_of_p = _pairs_per_row(A)
         c1, c2 = A.indices[first], A.indices[second]
         fac = A.data[first] * A.data[second]
@@ -220,16 +244,22 @@ class SpatioTemporalModel:
         # --- scratch
         self.nparts = 148
         self.part = torch.zeros(4096, **f64)
-        self.scal = torch.zeros(64, **f64)
-        self.coef_dev = torch.zeros((2 * n - 1) * 4, **f64)
-        self.coef_host = torch.zeros((2 * n - 1) * 4, dtype=torch.float64).pin_memory()
-        self.rhs = torch.zeros(self.N, **f64)
-        self.x = torch.zeros(self.N, **f64)  # latent mode / mean, like model.x
-        self.eta = torch.zeros(self.nobs, **f64)
         self.dvec = torch.zeros(self.nobs, **f64)
-        self.inner_c = torch.zeros((2 * n - 1) * 4, **f64)
-        self.inner_p = torch.zeros((2 * n - 1) * 4, **f64)
-        self.quad_st = torch.zeros((2 * n - 1) * 4, **f64)
+        self.slots = [self._new_slot(self.Qc, self.Qp)]
+
+    def _new_slot(self, Qc=None, Qp=None):
+        return _Slot(self.nt, self.ns, self.nb, self.N, self.nobs, self._dev, Qc, Qp)
+
+    def slot(self, j):
+        while len(self.slots) <= j:
+            self.slots.append(self._new_slot())
+        return self.slots[j]
+
+    # slot 0 carries the state of single-point evaluations (model.x, ...)
+    x = property(lambda self: self.slots[0].x)
+    rhs = property(lambda self: self.slots[0].rhs)
+    eta = property(lambda self: self.slots[0].eta)
+    scal = property(lambda self: self.slots[0].scal)
 
     # ------------------------------------------------------------------ host
     def coef_blocks(self, theta):
@@ -268,20 +298,21 @@ class SpatioTemporalModel:
     def _check(self, rc, what):
         _lib.check(rc, what)
 
-    def _assemble_prior(self, theta, M: BTAMatrix):
+    def _assemble_prior(self, theta, M: BTAMatrix, sl, which):
         c = np.asarray(self.coef_blocks(theta), dtype=np.float64).ravel()
-        self.coef_host.numpy()[:] = c
-        self.coef_dev.copy_(self.coef_host, non_blocking=True)
+        sl.coef_host[which].numpy()[:] = c
+        sl.coef_dev[which].copy_(sl.coef_host[which], non_blocking=True)
         D, L, _, _ = M.ptrs()
-        self._check(self.lib.bta_assemble_prior(self._stream(), M.n, M.b, _lib.ptr(self.coef_dev),
+        self._check(self.lib.bta_assemble_prior(self._stream(), M.n, M.b, _lib.ptr(sl.coef_dev[which]),
                                                 _lib.ptr(self.u_rowptr), _lib.ptr(self.u_col),
                                                 _lib.ptr(self.u_vals4), D, L), "assemble_prior")
 
-    def assemble_conditional(self, theta, d=None, dscale=1.0):
+    def assemble_conditional(self, theta, d=None, dscale=1.0, sl=None):
         """Q_c = Q_prior + A^T diag(dscale * d) A in BTA storage (``model.py:384-423``);
         d None means the Gaussian constant diagonal."""
-        Q = self.Qc
-        self._assemble_prior(theta, Q)
+        sl = self.slots[0] if sl is None else sl
+        Q = sl.Qc
+        self._assemble_prior(theta, Q, sl, 0)
         if Q.a > 0:
             Q.Ab.zero_()
         dptr = _lib.ptr(d)
@@ -293,8 +324,9 @@ class SpatioTemporalModel:
                                                self.fe_prec, float(dscale), _lib.ptr(self.part), self.nparts,
                                                _lib.ptr(Q.T)), "arrow_tip")
 
-    def assemble_prior_bt(self, theta):
-        self._assemble_prior(theta, self.Qp)
+    def assemble_prior_bt(self, theta, sl=None):
+        sl = self.slots[0] if sl is None else sl
+        self._assemble_prior(theta, sl.Qp, sl, 1)
 
     def factor(self, M: BTAMatrix):
         D, L, Ab, T = M.ptrs()
@@ -325,11 +357,10 @@ class SpatioTemporalModel:
         self._check(self.lib.bta_pobtasi_batched(self.h.bind_stream(), k, n, b, a, D, L, Ab, T),
                     "pobtasi_batched")
 
-    def logdet_to(self, M: BTAMatrix, slot):
+    def logdet_to(self, M: BTAMatrix, out):
         D, _, _, T = M.ptrs()
-        out = _lib.ptr(self.scal[slot:slot + 1])
-        self._check(self.lib.bta_logdet(self.h.bind_stream(), M.n, M.b, M.a, D, T, 1 if M.a else 0, out, None),
-                    "logdet")
+        self._check(self.lib.bta_logdet(self.h.bind_stream(), M.n, M.b, M.a, D, T, 1 if M.a else 0, _lib.ptr(out),
+                                        None), "logdet")
 
     def sweep(self, M: BTAMatrix, x, trans):
         D, L, Ab, T = M.ptrs()
@@ -340,9 +371,15 @@ class SpatioTemporalModel:
         D, L, Ab, T = M.ptrs()
         self._check(self.lib.bta_pobtasi(self.h.bind_stream(), M.n, M.b, M.a, D, L, Ab, T), "pobtasi")
 
-    def dot_to(self, x, y, slot):
+    def dot_to(self, x, y, out):
         self._check(self.lib.bta_dot(self._stream(), x.numel(), _lib.ptr(x), _lib.ptr(y), _lib.ptr(self.part),
-                                     self.nparts, _lib.ptr(self.scal[slot:slot + 1])), "dot")
+                                     self.nparts, _lib.ptr(out)), "dot")
+
+    def sweep_batched(self, mats, xs, trans):
+        k, n, b, a, D, L, Ab, T = self._batched_args(mats)
+        X = (ctypes.c_void_p * k)(*[x.data_ptr() for x in xs])
+        self._check(self.lib.bta_pobtas_batched(self.h.bind_stream(), k, n, b, a, D, L, Ab, T, X, trans),
+                    "pobtas_batched")
 
     def spmv(self, rowptr, col, val, m, x, y, alpha=1.0, beta=0.0):
         self._check(self.lib.bta_csr_spmv(self._stream(), m, _lib.ptr(rowptr), _lib.ptr(col), _lib.ptr(val),
@@ -361,22 +398,23 @@ class SpatioTemporalModel:
         theta = np.asarray(theta, dtype=np.float64)
         _lib.check(self.lib.bta_reset_status(self.h.bind_stream()), "reset")
         if self.gaussian:
+            sl = self.slots[0]
             tau = math.exp(theta[-1])
-            self.assemble_conditional(theta, None, tau)
-            self.factor(self.Qc)
-            self.logdet_to(self.Qc, 0)
+            self.assemble_conditional(theta, None, tau, sl)
+            self.factor(sl.Qc)
+            self.logdet_to(sl.Qc, sl.scal[0:1])
             # rhs = -Q_prior x + A^T grad(lik) at x = 0, eta = 0  ->  tau A^T y
             self._check(self.lib.bta_axpby(self._stream(), self.N, tau, _lib.ptr(self.Aty), 0.0,
-                                           _lib.ptr(self.rhs)), "axpby")
-            self.x.copy_(self.rhs)
-            self.sweep(self.Qc, self.x, 0)
-            self.sweep(self.Qc, self.x, 1)
-            self.dot_to(self.rhs, self.x, 1)  # mu^T Q_c mu = b^T mu
-            self.assemble_prior_bt(theta)
-            self.factor(self.Qp)
-            self.logdet_to(self.Qp, 2)
+                                           _lib.ptr(sl.rhs)), "axpby")
+            sl.x.copy_(sl.rhs)
+            self.sweep(sl.Qc, sl.x, 0)
+            self.sweep(sl.Qc, sl.x, 1)
+            self.dot_to(sl.rhs, sl.x, sl.scal[1:2])  # mu^T Q_c mu = b^T mu
+            self.assemble_prior_bt(theta, sl)
+            self.factor(sl.Qp)
+            self.logdet_to(sl.Qp, sl.scal[2:3])
             self.status()
-            s = self.scal[:3].cpu().numpy()
+            s = sl.scal[:3].cpu().numpy()
             cond = 0.5 * s[0] - 0.5 * s[1]
             f = cond - (self.log_prior_theta(theta) + self.lik0(theta) + 0.5 * s[2])
         else:
@@ -411,8 +449,14 @@ class SpatioTemporalModel:
         return float(np.imag(fun(th)) / _CSTEP)
 
     def objective_adjoint(self, theta):
-        """(f, exact gradient) from one factorisation + selected inversion of
-        Q_c and of Q_prior:
+        """(f, exact gradient) at one theta, see ``objective_adjoint_batched``."""
+        f, g = self.objective_adjoint_batched([theta])
+        return f[0], g[0]
+
+    def objective_adjoint_batched(self, thetas):
+        """(f, exact gradient) at K theta points (e.g. the candidates of a line
+        search), factorising and selected-inverting all 2K matrices (Q_c and
+        Q_prior of every point) together:
         df/dth = 1/2 tr(S_c dQ_c) - 1/2 tr(S_p dQ_st) + 1/2 mu^T dQ_c mu
                  - mu^T db - d log p(theta) - d lik0,
         with tr(S dQ_st) and mu^T dQ_st mu contracted block by block against
@@ -420,58 +464,67 @@ class SpatioTemporalModel:
         pattern (Gaussian likelihood)."""
         if not self.gaussian:
             raise NotImplementedError("adjoint gradient: Gaussian likelihood")
-        import torch
-
-        theta = np.asarray(theta, dtype=np.float64)
+        thetas = [np.asarray(t, dtype=np.float64) for t in thetas]
+        K = len(thetas)
         n, b, a = self.nt, self.ns, self.nb
-        tau = math.exp(theta[-1])
         stream = self._stream()
+        sls = [self.slot(j) for j in range(K)]
+        taus = [math.exp(t[-1]) for t in thetas]
         _lib.check(self.lib.bta_reset_status(self.h.bind_stream()), "reset")
-        self.assemble_conditional(theta, None, tau)
-        self.assemble_prior_bt(theta)
-        self.factor_batched([self.Qc, self.Qp])
-        self.logdet_to(self.Qc, 0)
-        self.logdet_to(self.Qp, 2)
-        self._check(self.lib.bta_axpby(stream, self.N, tau, _lib.ptr(self.Aty), 0.0, _lib.ptr(self.rhs)), "axpby")
-        self.x.copy_(self.rhs)
-        self.sweep(self.Qc, self.x, 0)
-        self.dot_to(self.x, self.x, 1)  # b^T Q^-1 b = |L^-1 b|^2
-        self.sweep(self.Qc, self.x, 1)  # mu
-        # |A mu|^2 and mu^T (E_tt' (x) K) mu
-        self.spmv(self.A_rowptr, self.A_col, self.A_val, self.nobs, self.x, self.eta)
-        self.dot_to(self.eta, self.eta, 3)
-        self._check(self.lib.bta_block_quad(stream, n, b, _lib.ptr(self.u_rowptr), _lib.ptr(self.u_col),
-                                            _lib.ptr(self.u_vals4), _lib.ptr(self.x), _lib.ptr(self.quad_st)),
-                    "block_quad")
+        for sl, th, tau in zip(sls, thetas, taus):
+            self.assemble_conditional(th, None, tau, sl)
+            self.assemble_prior_bt(th, sl)
+        self.factor_batched([sl.Qc for sl in sls] + [sl.Qp for sl in sls])
+        for sl, tau in zip(sls, taus):
+            self.logdet_to(sl.Qc, sl.scal[0:1])
+            self.logdet_to(sl.Qp, sl.scal[2:3])
+            self._check(self.lib.bta_axpby(stream, self.N, tau, _lib.ptr(self.Aty), 0.0, _lib.ptr(sl.rhs)), "axpby")
+            sl.x.copy_(sl.rhs)
+        self.sweep_batched([sl.Qc for sl in sls], [sl.x for sl in sls], 0)
+        for sl in sls:
+            self.dot_to(sl.x, sl.x, sl.scal[1:2])  # b^T Q^-1 b = |L^-1 b|^2
+        self.sweep_batched([sl.Qc for sl in sls], [sl.x for sl in sls], 1)  # mu
+        for sl in sls:
+            # |A mu|^2 and mu^T (E_tt' (x) K) mu
+            self.spmv(self.A_rowptr, self.A_col, self.A_val, self.nobs, sl.x, sl.eta)
+            self.dot_to(sl.eta, sl.eta, sl.scal[3:4])
+            self._check(self.lib.bta_block_quad(stream, n, b, _lib.ptr(self.u_rowptr), _lib.ptr(self.u_col),
+                                                _lib.ptr(self.u_vals4), _lib.ptr(sl.x), _lib.ptr(sl.quad_st)),
+                        "block_quad")
         # selected inverses and their contractions
-        self.selinv_batched([self.Qc, self.Qp])
-        Dc, Lc, _, _ = self.Qc.ptrs()
-        Dp, Lp, _, _ = self.Qp.ptrs()
-        for (Dm, Lm, out) in ((Dc, Lc, self.inner_c), (Dp, Lp, self.inner_p)):
-            self._check(self.lib.bta_block_inner(stream, n, b, _lib.ptr(self.u_rowptr), _lib.ptr(self.u_col),
-                                                 _lib.ptr(self.u_vals4), Dm, Lm, _lib.ptr(out)), "block_inner")
-        self._check(self.lib.bta_gather_dot(stream, self.nent, _lib.ptr(self.ent_dst), _lib.ptr(self.ata_w),
-                                            _lib.ptr(self.Qc.buf), _lib.ptr(self.part), self.nparts,
-                                            _lib.ptr(self.scal[4:5])), "gather_dot")
+        self.selinv_batched([sl.Qc for sl in sls] + [sl.Qp for sl in sls])
+        for sl in sls:
+            Dc, Lc, _, _ = sl.Qc.ptrs()
+            Dp, Lp, _, _ = sl.Qp.ptrs()
+            for (Dm, Lm, out) in ((Dc, Lc, sl.inner_c), (Dp, Lp, sl.inner_p)):
+                self._check(self.lib.bta_block_inner(stream, n, b, _lib.ptr(self.u_rowptr), _lib.ptr(self.u_col),
+                                                     _lib.ptr(self.u_vals4), Dm, Lm, _lib.ptr(out)), "block_inner")
+            self._check(self.lib.bta_gather_dot(stream, self.nent, _lib.ptr(self.ent_dst), _lib.ptr(self.ata_w),
+                                                _lib.ptr(sl.Qc.buf), _lib.ptr(self.part), self.nparts,
+                                                _lib.ptr(sl.scal[4:5])), "gather_dot")
         self.status()
-        s = self.scal[:5].cpu().numpy()
-        Ic = self.inner_c.view(-1, 4).cpu().numpy()
-        Ip = self.inner_p.view(-1, 4).cpu().numpy()
-        Qm = self.quad_st.view(-1, 4).cpu().numpy()
-        Tsel = self.Qc.T.cpu().numpy()
         mult = np.ones((2 * n - 1, 1))
         mult[n:] = 2.0  # each sub-diagonal block appears twice in the symmetric matrix
-        f = 0.5 * s[0] - 0.5 * s[1] - (self.log_prior_theta(theta) + self.lik0(theta) + 0.5 * s[2])
-        grad = np.zeros(theta.size)
-        for k in range(3):
-            dc = self._dcoef(theta, k) * mult
-            grad[k] = (0.5 * np.sum(dc * Ic) - 0.5 * np.sum(dc * Ip) + 0.5 * np.sum(dc * Qm)
-                       - self._dfun(self.log_prior_theta, theta, k))
-        tr_ata = s[4] + float(np.sum(Tsel * self.XtX_host))
-        grad[-1] = (0.5 * tau * tr_ata - s[1] + 0.5 * tau * s[3]
-                    - (0.5 * self.nobs - 0.5 * tau * self.yty)
-                    - self._dfun(self.log_prior_theta, theta, theta.size - 1))
-        return float(f), grad
+        fs, grads = [], []
+        for sl, theta, tau in zip(sls, thetas, taus):
+            s = sl.scal[:5].cpu().numpy()
+            Ic = sl.inner_c.view(-1, 4).cpu().numpy()
+            Ip = sl.inner_p.view(-1, 4).cpu().numpy()
+            Qm = sl.quad_st.view(-1, 4).cpu().numpy()
+            Tsel = sl.Qc.T.cpu().numpy()
+            f = 0.5 * s[0] - 0.5 * s[1] - (self.log_prior_theta(theta) + self.lik0(theta) + 0.5 * s[2])
+            grad = np.zeros(theta.size)
+            for k in range(3):
+                dc = self._dcoef(theta, k) * mult
+                grad[k] = (0.5 * np.sum(dc * Ic) - 0.5 * np.sum(dc * Ip) + 0.5 * np.sum(dc * Qm)
+                           - self._dfun(self.log_prior_theta, theta, k))
+            tr_ata = s[4] + float(np.sum(Tsel * self.XtX_host))
+            grad[-1] = (0.5 * tau * tr_ata - s[1] + 0.5 * tau * s[3]
+                        - (0.5 * self.nobs - 0.5 * tau * self.yty)
+                        - self._dfun(self.log_prior_theta, theta, theta.size - 1))
+            fs.append(float(f))
+            grads.append(grad)
+        return fs, grads
 
     # ------------------------------------------------------------- Poisson
     def _evaluate_f_poisson(self, theta):

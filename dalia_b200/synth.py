@@ -213,6 +213,8 @@ def make_problem(
 CONFIGS = {
     "gst_300x10": dict(ns=300, nt=10, nb=4, no=200, theta=(-1.0, 1.0, 0.0, 2.0), likelihood="gaussian"),
     "gst_1500x100": dict(ns=1500, nt=100, nb=6, no=600, theta=(-1.0, 1.0, 0.0, 2.0), likelihood="gaussian"),
+    # same model on 20 time steps: a mid-size case (BTA factor 0.7 GB) for profiling
+    "gst_1500x20": dict(ns=1500, nt=20, nb=6, no=600, theta=(-1.0, 1.0, 0.0, 2.0), likelihood="gaussian"),
     "pst_2500x60": dict(ns=2500, nt=60, nb=6, no=800, theta=(-1.2, 0.8, -0.3), likelihood="poisson"),
     "gst_4000x250": dict(ns=4000, nt=250, nb=6, no=1500, theta=(-1.0, 1.0, 0.0, 2.0), likelihood="gaussian"),
 }

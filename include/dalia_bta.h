@@ -65,10 +65,14 @@ int bta_pobtaf(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, doubl
  * launch.  This is the batched launch over the theta points of a
  * finite-difference stencil or a line search (the reference evaluates them one
  * after another, src/dalia/core/dalia.py:558-564).  For the batched
- * factorisation, info = k * 2^40 + pivot identifies instance k.
+ * factorisation, info = k * 2^40 + pivot identifies instance k.  The batched
+ * sweep takes up to 32 instances, each with its own right-hand side rhs[k].
  */
 int bta_pobtaf_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
                        double* const* D, double* const* L, double* const* Ab, double* const* T, int64_t* info);
+int bta_pobtas_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                       const double* const* D, const double* const* L, const double* const* Ab,
+                       const double* const* T, double* const* rhs, int trans);
 int bta_pobtasi_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
                         double* const* D, double* const* L, double* const* Ab, double* const* T);
 

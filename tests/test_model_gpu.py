@@ -48,3 +48,16 @@ def test_adjoint_gradient(name):
     if prob.ns * prob.nt <= 400:
         ga = model_ref.dense_adjoint_gradient(model_ref.OracleModel(prob), g["theta"])
         assert rel(grad, ga) < 1e-9
+
+
+def test_batched_adjoint_matches_single_points():
+    from dalia_b200.model import SpatioTemporalModel
+
+    g = load("gst_ragged")
+    m = SpatioTemporalModel(problem(g))
+    thetas = [g["theta"] + d for d in (0.0, 0.01, -0.02)]
+    fs, gs = m.objective_adjoint_batched(thetas)
+    for th, f, gr in zip(thetas, fs, gs):
+        f1, g1 = m.objective_adjoint(th)
+        assert abs(f - f1) < 1e-10 * abs(f1)
+        assert rel(gr, g1) < 1e-10
