@@ -28,6 +28,7 @@ _i64 = ctypes.c_int64
 _int = ctypes.c_int
 _pi64 = ctypes.POINTER(ctypes.c_int64)
 _pdbl = ctypes.POINTER(ctypes.c_double)
+_dbl = ctypes.c_double
 
 SIGNATURES = {
     "bta_create": (_int, [ctypes.POINTER(_c_void_p)]),
@@ -66,6 +67,14 @@ SIGNATURES = {
                                _c_void_p]),
     "bta_block_quad": (_int, [_c_void_p, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p]),
     "bta_gather_dot": (_int, [_c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _int, _c_void_p]),
+    "bta_kron_symv": (_int, [_c_void_p, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _dbl,
+                             _dbl, _c_void_p]),
+    "bta_poisson_terms": (_int, [_c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                 _int, _c_void_p]),
+    "bta_block_bilinear": (_int, [_c_void_p, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                  _c_void_p]),
+    "bta_obs_quad": (_int, [_c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _i64, _c_void_p, _c_void_p,
+                            _c_void_p, _c_void_p]),
     "bta_csr_spmv": (_int, [_c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, ctypes.c_double,
                             ctypes.c_double, _c_void_p]),
     "bta_symv": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,

@@ -267,6 +267,122 @@ __global__ void axpby_kernel(int64_t n, double alpha, const double* x, double be
     y[i] = alpha * x[i] + (beta != 0.0 ? beta * y[i] : 0.0);
 }
 
+// y_r = alpha * (Q_st x)_r + beta * y_r for every row r = t*b + s of the
+// spatio-temporal block: the row meets the blocks (t, t-1), (t, t) and
+// (t, t+1) = (t+1, t)^T, each sum_K coef[blk][K] K (K symmetric).  One warp
+// per row; lanes stride the union pattern of the spatial row s.
+__global__ void __launch_bounds__(256) kron_symv_kernel(int n, int b, const double* coef, const int* rowptr,
+                                                        const int* colidx, const double* vals4, const double* x,
+                                                        double alpha, double beta, double* y) {
+  const int lane = threadIdx.x & 31;
+  const int64_t rows = (int64_t)n * b;
+  for (int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; r < rows;
+       r += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    const int t = (int)(r / b), s = (int)(r - (int64_t)t * b);
+    const double* cd = coef + (size_t)t * 4;
+    const double* cl = t > 0 ? coef + (size_t)(n + t - 1) * 4 : nullptr;
+    const double* cu = t < n - 1 ? coef + (size_t)(n + t) * 4 : nullptr;
+    const double* x0 = x + (size_t)t * b;
+    double acc = 0.0;
+    for (int e = rowptr[s] + lane; e < rowptr[s + 1]; e += 32) {
+      const int c = colidx[e];
+      const double* v = vals4 + (size_t)e * 4;
+      const double v0 = v[0], v1 = v[1], v2 = v[2], v3 = v[3];
+      acc += (cd[0] * v0 + cd[1] * v1 + cd[2] * v2 + cd[3] * v3) * x0[c];
+      if (cl) acc += (cl[0] * v0 + cl[1] * v1 + cl[2] * v2 + cl[3] * v3) * x0[c - b];
+      if (cu) acc += (cu[0] * v0 + cu[1] * v1 + cu[2] * v2 + cu[3] * v3) * x0[c + b];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) y[r] = alpha * acc + (beta != 0.0 ? beta * y[r] : 0.0);
+  }
+}
+
+// Poisson terms at eta: d = e exp(eta) (minus the likelihood Hessian diagonal),
+// g = y - d (likelihood gradient), part[blockIdx] = partial sum of eta y - d.
+__global__ void __launch_bounds__(256) poisson_terms_kernel(int64_t m, const double* eta, const double* y,
+                                                            const double* e, double* d, double* g, double* part) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+    const double et = eta[i];
+    const double di = e[i] * exp(et);
+    d[i] = di;
+    g[i] = y[i] - di;
+    s += et * y[i] - di;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// out[blk][K] = u_t^T K x_t (diagonal block t = blk < n) or
+// u_{t+1}^T K x_t + u_t^T K x_{t+1} (sub-diagonal block t = blk - n): the
+// bilinear form u^T (E (x) K) x of the symmetric Kronecker block pair.
+__global__ void __launch_bounds__(256) block_bilinear_kernel(int n, int b, const int* rowptr, const int* colidx,
+                                                             const double* vals4, const double* u, const double* x,
+                                                             double* out) {
+  __shared__ double red[4][256];
+  const int blk = blockIdx.x;
+  const bool lower = blk >= n;
+  const int t = lower ? blk - n : blk;
+  const double* ur = u + (size_t)(lower ? t + 1 : t) * b;
+  const double* xc = x + (size_t)t * b;
+  const double* ur2 = u + (size_t)t * b;
+  const double* xc2 = x + (size_t)(t + 1) * b;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int row = threadIdx.x; row < b; row += blockDim.x) {
+    const double uv = ur[row];
+    const double uv2 = lower ? ur2[row] : 0.0;
+    for (int e = rowptr[row]; e < rowptr[row + 1]; ++e) {
+      const int c = colidx[e];
+      const double m = uv * xc[c] + (lower ? uv2 * xc2[c] : 0.0);
+      const double* v = vals4 + (size_t)e * 4;
+      s[0] += m * v[0];
+      s[1] += m * v[1];
+      s[2] += m * v[2];
+      s[3] += m * v[3];
+    }
+  }
+  for (int k = 0; k < 4; ++k) red[k][threadIdx.x] = s[k];
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int k = 0; k < 4; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) out[(size_t)blk * 4 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// out[i] = scale[i] * (a_i^T S a_i) for every observation row a_i of A, with
+// S on the BTA pattern: the (entry, weight) pairs of row i (off/dst/w, weights
+// already doubled for entries of L and Ab blocks) plus the fixed-effect part
+// x_i^T T x_i (X: nobs x a, row-major).  One warp per observation.
+__global__ void __launch_bounds__(256) obs_quad_kernel(int64_t nobs, const int64_t* off, const int64_t* dst,
+                                                       const double* w, const double* base, int a, const double* X,
+                                                       const double* T, const double* scale, double* out) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < nobs;
+       i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    double s = 0.0;
+    for (int64_t j = off[i] + lane; j < off[i + 1]; j += 32) s += w[j] * base[dst[j]];
+    if (a > 0) {
+      const double* xi = X + (size_t)i * a;
+      for (int pq = lane; pq < a * a; pq += 32) {
+        const int p = pq / a, q = pq - p * a;
+        s += xi[p] * xi[q] * T[pq];
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) out[i] = scale ? scale[i] * s : s;
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -390,6 +506,57 @@ int bta_symv(void* stream, int64_t n, int64_t b, int64_t a, const double* D, con
     bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
     bta_symv_kernel<<<(int)((rows + 7) / 8), 256, 0, (cudaStream_t)stream>>>((int)n, (int)b, (int)a, D, L, Ab, T, x,
                                                                             y);
+  }
+  return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
+}
+
+int bta_kron_symv(void* stream, int64_t n, int64_t b, const double* coef, const int* rowptr, const int* colidx,
+                  const double* vals4, const double* x, double alpha, double beta, double* y) {
+  if (n < 1 || b < 1 || !coef || !rowptr || !colidx || !vals4 || !x || !y) return BTA_ERR_INVALID;
+  const int64_t rows = n * b;
+  const int grid = (int)std::min<int64_t>((rows * 32 + 255) / 256, 148 * 32);
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    kron_symv_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>((int)n, (int)b, coef, rowptr, colidx, vals4, x, alpha,
+                                                             beta, y);
+  }
+  return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
+}
+
+int bta_poisson_terms(void* stream, int64_t nobs, const double* eta, const double* y, const double* e, double* d,
+                      double* g, double* part, int nparts, double* lik) {
+  if (nobs < 0 || nparts < 1 || !part || !lik || (nobs > 0 && (!eta || !y || !e || !d || !g)))
+    return BTA_ERR_INVALID;
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    poisson_terms_kernel<<<nparts, 256, 0, (cudaStream_t)stream>>>(nobs, eta, y, e, d, g, part);
+  }
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    sum_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(part, nparts, lik);
+  }
+  return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
+}
+
+int bta_block_bilinear(void* stream, int64_t n, int64_t b, const int* rowptr, const int* colidx, const double* vals4,
+                       const double* u, const double* x, double* out) {
+  if (n < 1 || b < 1 || !rowptr || !colidx || !vals4 || !u || !x || !out) return BTA_ERR_INVALID;
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    block_bilinear_kernel<<<(int)(2 * n - 1), 256, 0, (cudaStream_t)stream>>>((int)n, (int)b, rowptr, colidx, vals4,
+                                                                            u, x, out);
+  }
+  return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
+}
+
+int bta_obs_quad(void* stream, int64_t nobs, const int64_t* off, const int64_t* dst, const double* w,
+                 const double* base, int64_t a, const double* X, const double* T, const double* scale, double* out) {
+  if (nobs < 0 || a < 0 || (nobs > 0 && (!off || !out || !base)) || (a > 0 && (!X || !T))) return BTA_ERR_INVALID;
+  if (nobs == 0) return BTA_OK;
+  const int grid = (int)std::min<int64_t>((nobs * 32 + 255) / 256, 148 * 32);
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    obs_quad_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(nobs, off, dst, w, base, (int)a, X, T, scale, out);
   }
   return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
 }

@@ -46,6 +46,33 @@ int bta_block_inner(void* stream, int64_t n, int64_t b, const int* rowptr, const
 int bta_block_quad(void* stream, int64_t n, int64_t b, const int* rowptr, const int* colidx,
                    const double* vals4, const double* x, double* out);
 
+/* y[0 : n*b] = alpha * Q_st x + beta * y[0 : n*b]: the spatio-temporal block
+ * applied through its Kronecker structure (coef and the union pattern as in
+ * bta_assemble_prior); the product -Q_prior x of the reference's information
+ * vector (src/dalia/core/model.py:425-449) without forming Q_prior. */
+int bta_kron_symv(void* stream, int64_t n, int64_t b, const double* coef, const int* rowptr, const int* colidx,
+                  const double* vals4, const double* x, double alpha, double beta, double* y);
+
+/* Poisson likelihood at eta (src/dalia/likelihoods/poisson.py:35-63):
+ * d = e exp(eta) (minus the Hessian diagonal), g = y - d (gradient),
+ * *lik = eta . y - sum(e exp(eta)). */
+int bta_poisson_terms(void* stream, int64_t nobs, const double* eta, const double* y, const double* e, double* d,
+                      double* g, double* part, int nparts, double* lik);
+
+/* out[blk][K] = u_t^T K x_t (blk = t < n) or u_{t+1}^T K x_t + u_t^T K x_{t+1}
+ * (blk = n + t): u^T dQ_st x for Kronecker-structured dQ_st. */
+int bta_block_bilinear(void* stream, int64_t n, int64_t b, const int* rowptr, const int* colidx, const double* vals4,
+                       const double* u, const double* x, double* out);
+
+/* out[i] = scale[i] * a_i^T S a_i (scale NULL means 1) for every row a_i of
+ * A = [A_st | X], with S on the BTA pattern given by per-observation entry
+ * lists (off[nobs+1], dst = element offsets into base, w = weight products,
+ * doubled for L and Ab entries) and the tip T (a x a) with the dense rows of
+ * X: diag(A S A^T), the observation marginal variances of
+ * src/dalia/core/dalia.py:964-1021 when S = Q_c^{-1}. */
+int bta_obs_quad(void* stream, int64_t nobs, const int64_t* off, const int64_t* dst, const double* w,
+                 const double* base, int64_t a, const double* X, const double* T, const double* scale, double* out);
+
 /* *out = sum_e w[e] * base[idx[e]] */
 int bta_gather_dot(void* stream, int64_t nent, const int64_t* idx, const double* w, const double* base,
                    double* part, int nparts, double* out);

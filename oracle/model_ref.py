@@ -300,3 +300,37 @@ def dense_adjoint_gradient(model: OracleModel, theta):
     grad[-1] = (0.5 * np.sum(Sc * dQc) + 0.5 * mu @ dQc @ mu - mu @ b - dlik
                 - _cstep(lambda th: _log_prior_complex(model, th), theta, theta.size - 1))
     return grad
+
+
+def dense_adjoint_gradient_poisson(model: OracleModel, theta):
+    """Dense restatement of the GPU Poisson adjoint gradient: the Newton
+    iteration of ``OracleModel.inner_iteration`` (warm started from
+    ``model.x``) gives x*, eta = A x* and Q_c; dx is the final Newton update
+    (not applied, as in the reference), S_c = Q_c^{-1}, S_p = Q_st^{-1},
+    d = e exp(eta), z = S_c A^T (d * diag(A S_c A^T)):
+      df/dth_k = 1/2 x*^T dQ x* + 1/2 tr(S_c dQ) - 1/2 tr(S_p dQ_st)
+                 + (dx - z/2)^T dQ x* - d log p(theta)."""
+    theta = np.asarray(theta, dtype=np.float64)
+    assert not model.gaussian
+    nst = model.ns * model.nt
+    Qc_sp, xs, eta = model.inner_iteration(theta)
+    model.x[:] = xs
+    Qc = Qc_sp.toarray()
+    Qp = model.q_prior(theta).toarray()
+    Ad = model.A.toarray()
+    rhs = -Qp @ xs + Ad.T @ model.grad_lik(theta, eta)
+    dx = np.linalg.solve(Qc, rhs)
+    Sc = np.linalg.inv(Qc)
+    Sp = np.linalg.inv(model.q_st(theta).toarray())
+    d = model.e * np.exp(eta)
+    h = d * np.einsum("ij,jk,ik->i", Ad, Sc, Ad)
+    z = Sc @ (Ad.T @ h)
+    u = dx - 0.5 * z
+    grad = np.zeros(theta.size)
+    for k in range(theta.size):
+        dQ = _cstep(lambda th: _q_st_complex(model, th), theta, k)
+        dQc = np.zeros_like(Qc)
+        dQc[:nst, :nst] = dQ
+        grad[k] = (0.5 * xs @ dQc @ xs + 0.5 * np.sum(Sc * dQc) - 0.5 * np.sum(Sp * dQ) + u @ dQc @ xs
+                   - _cstep(lambda th: _log_prior_complex(model, th), theta, k))
+    return grad

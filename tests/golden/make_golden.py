@@ -3,7 +3,7 @@
 
 Usage (needs the reference checkout; it is not needed to *use* the fixtures)::
 
-    ARRAY_MODULE=numpy python tests/golden/make_golden.py /path/to/DALIA
+    ARRAY_MODULE=numpy python tests/golden/make_golden.py /path/to/DALIA [CASE ...]
 
 For every case the reference's own classes are driven end to end:
 
@@ -42,6 +42,7 @@ CASES = {
     "gst_ragged": (70, 3, 2, 50, (-0.5, 0.7, 0.2, 1.5), "gaussian", 2, True),
     "pst_small": (40, 4, 2, 60, (-1.2, 0.8, -0.3), "poisson", 3, False),
     "gst_300x10": (300, 10, 4, 200, (-1.0, 1.0, 0.0, 2.0), "gaussian", 0, False),
+    "pst_150x6": (150, 6, 3, 120, (-1.0, 0.9, -0.2), "poisson", 4, False),
 }
 
 
@@ -55,7 +56,7 @@ def checksums(prob):
     return out
 
 
-def main(ref_root: str) -> None:
+def main(ref_root: str, only=None) -> None:
     os.environ.setdefault("ARRAY_MODULE", "numpy")
     sys.path.insert(0, REPO)
     sys.path.insert(0, os.path.join(ref_root, "src"))
@@ -86,6 +87,8 @@ def main(ref_root: str) -> None:
     SerinvSolver.cholesky = _chol_default
 
     for name, (ns, nt, nb, no, theta, lik, seed, store_selinv) in CASES.items():
+        if only and name not in only:
+            continue
         prob = synth.make_problem(ns, nt, nb, no, theta, lik, seed=seed)
         tmp = tempfile.mkdtemp(prefix=f"golden_{name}_")
         synth.save_dalia_layout(prob, tmp)
@@ -173,4 +176,5 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DALIA_REF", "/root/reference"))
+    # usage: make_golden.py [REF_ROOT [CASE ...]]
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DALIA_REF", "/root/reference"), sys.argv[2:])

@@ -8,6 +8,7 @@ from golden_util import load, problem, rel
 from oracle import bta_ref, model_ref
 
 GAUSS = ["gst_small", "gst_ragged"]
+POIS = ["pst_small", "pst_150x6"]
 
 
 @pytest.mark.parametrize("name", GAUSS)
@@ -41,7 +42,7 @@ def test_bta_oracle_matches_dense_lapack(name):
         assert rel(arr, g[k]) < 1e-10, k
 
 
-@pytest.mark.parametrize("name", GAUSS + ["pst_small"])
+@pytest.mark.parametrize("name", GAUSS + POIS)
 def test_objective_matches_reference_serinv_path(name):
     g = load(name)
     prob = problem(g)
@@ -52,7 +53,7 @@ def test_objective_matches_reference_serinv_path(name):
     assert rel(om.x, g["x_serinv"]) < 1e-10
 
 
-@pytest.mark.parametrize("name", GAUSS + ["pst_small"])
+@pytest.mark.parametrize("name", GAUSS + POIS)
 def test_serinv_and_dense_paths_differ_by_tip_constant(name):
     """Reference quirk: the Serinv path's prior log-determinant drops the
     fixed-effect tip, so f differs from the dense path by -0.5 nb log(1e-3)."""
@@ -94,3 +95,21 @@ def test_dense_adjoint_matches_reference_fd_gradient(name):
     om.eps = 1e-5
     _, gfd = om.objective(g["theta"])
     assert rel(ga, gfd) < 1e-7
+
+
+@pytest.mark.parametrize("name", POIS)
+def test_dense_poisson_adjoint_matches_fd_at_the_mode(name):
+    """With a tight Newton tolerance (x* = the mode) the Poisson adjoint
+    formula equals a fine central FD of the oracle objective."""
+    g = load(name)
+    prob = problem(g)
+    th = g["theta"]
+    om = model_ref.OracleModel(prob, eps_inner_iteration=1e-11)
+    ga = model_ref.dense_adjoint_gradient_poisson(om, th)
+    h = 1e-5
+    fd = []
+    for k in range(th.size):
+        e = np.zeros(th.size)
+        e[k] = h
+        fd.append((om.evaluate_f(th + e) - om.evaluate_f(th - e)) / (2 * h))
+    assert rel(ga, fd) < 1e-7
