@@ -97,6 +97,22 @@ def _pairs_per_row(A):
     return first, second, row_of_p
 
 
+def factor_flops(n, b, a):
+    """Algorithmic flops of one BTA factorisation (pobtaf): per block column
+    POTRF b^3/3, TRSM of the block below b^3 and of the arrow a b^2, the
+    previous column's Schur update b^3 (SYRK, lower half), 2 a b^2 (arrow)
+    and a^2 b (tip); plus the tip POTRF a^3/3."""
+    f = n * (b ** 3 / 3 + a * b ** 2 + a * a * b) + (n - 1) * (b ** 3 + b ** 3 + 2 * a * b ** 2)
+    return f + a ** 3 / 3
+
+
+def selinv_gemm_flops(n, b, a):
+    """Flops of the GEMMs of one selected inversion (pobtasi), per block
+    column: G = L Linv (b^3), S_{i+1,i} = -S G (2 b^3), S_ii (b^3/3 + b^3),
+    and the arrow terms."""
+    return (n - 1) * (4 * b ** 3 + 6 * a * b ** 2) + n * (b ** 3 / 3 + 4 * a * b ** 2 + 4 * a * a * b)
+
+
 class BTAMatrix:
     """One BTA matrix in a single device allocation with D, L, Ab, T views."""
 
@@ -261,6 +277,9 @@ class SpatioTemporalModel:
         self.part = torch.zeros(4096, **f64)
         self.dvec = torch.zeros(self.nobs, **f64)
         self.slots = [self._new_slot(self.Qc, self.Qp)]
+        # algorithmic flops of the factorisations / selected-inversion GEMMs
+        # issued so far, and Newton steps taken (non-Gaussian likelihoods)
+        self.work = {"factor": 0.0, "selinv_gemm": 0.0, "newton_steps": 0}
 
     def _new_slot(self, Qc=None, Qp=None):
         return _Slot(self.nt, self.ns, self.nb, self.N, self.nobs, self._dev, Qc, Qp)
@@ -344,6 +363,7 @@ class SpatioTemporalModel:
         self._assemble_prior(theta, sl.Qp, sl, 1)
 
     def factor(self, M: BTAMatrix):
+        self.work["factor"] += factor_flops(M.n, M.b, M.a)
         D, L, Ab, T = M.ptrs()
         self._check(self.lib.bta_pobtaf(self.h.bind_stream(), M.n, M.b, M.a, D, L, Ab, T, None), "pobtaf")
 
@@ -363,11 +383,13 @@ class SpatioTemporalModel:
 
     def factor_batched(self, mats):
         """All matrices factored together, block column by block column."""
+        self.work["factor"] += sum(factor_flops(m.n, m.b, m.a) for m in mats)
         k, n, b, a, D, L, Ab, T = self._batched_args(mats)
         self._check(self.lib.bta_pobtaf_batched(self.h.bind_stream(), k, n, b, a, D, L, Ab, T, None),
                     "pobtaf_batched")
 
     def selinv_batched(self, mats):
+        self.work["selinv_gemm"] += sum(selinv_gemm_flops(m.n, m.b, m.a) for m in mats)
         k, n, b, a, D, L, Ab, T = self._batched_args(mats)
         self._check(self.lib.bta_pobtasi_batched(self.h.bind_stream(), k, n, b, a, D, L, Ab, T),
                     "pobtasi_batched")
@@ -383,6 +405,7 @@ class SpatioTemporalModel:
                     "pobtas")
 
     def selinv(self, M: BTAMatrix):
+        self.work["selinv_gemm"] += selinv_gemm_flops(M.n, M.b, M.a)
         D, L, Ab, T = M.ptrs()
         self._check(self.lib.bta_pobtasi(self.h.bind_stream(), M.n, M.b, M.a, D, L, Ab, T), "pobtasi")
 
@@ -653,6 +676,7 @@ class SpatioTemporalModel:
             still = []
             for j, v in zip(active, nrm):
                 counter[j] += 1
+                self.work["newton_steps"] += 1
                 if math.sqrt(max(float(v), 0.0)) >= self.eps_inner:
                     still.append(j)
             active = still
