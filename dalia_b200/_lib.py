@@ -30,6 +30,9 @@ _pi64 = ctypes.POINTER(ctypes.c_int64)
 _pdbl = ctypes.POINTER(ctypes.c_double)
 _dbl = ctypes.c_double
 
+BTA_PREC_FP64 = 0
+BTA_PREC_TF32X3 = 1
+
 SIGNATURES = {
     "bta_create": (_int, [ctypes.POINTER(_c_void_p)]),
     "bta_destroy": (_int, [_c_void_p]),
@@ -44,6 +47,10 @@ SIGNATURES = {
                                   _c_void_p, _c_void_p, _int]),
     "bta_pobtasi_batched": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
                                    _c_void_p, _c_void_p]),
+    "bta_pobtasi_batched_ex": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                      _c_void_p, _c_void_p, _int]),
+    "bta_gemm": (_int, [_c_void_p, _int, _i64, _i64, _i64, _dbl, _c_void_p, _i64, _int, _c_void_p, _i64, _int,
+                        _dbl, _c_void_p, _i64, _int, _int]),
     "bta_pobtasi": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p]),
     "bta_logdet": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _int, _c_void_p, _pdbl]),
     "bta_get_status": (_int, [_c_void_p, _pi64]),

@@ -395,7 +395,18 @@ int bta_pobtas(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D,
 
 int bta_pobtasi_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
                         double* const* D, double* const* L, double* const* Ab, double* const* T) {
+  return bta_pobtasi_batched_ex(h, count, n, b, a, D, L, Ab, T, BTA_PREC_FP64);
+}
+
+int bta_pobtasi_batched_ex(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                           double* const* D, double* const* L, double* const* Ab, double* const* T,
+                           int precision) {
   if (!h || count < 1 || !n || !b || !a || !D) return BTA_ERR_INVALID;
+  if (precision != BTA_PREC_FP64 && precision != BTA_PREC_TF32X3) return BTA_ERR_INVALID;
+  // the b x b block products go to the tensor-core kernel in TF32x3 mode
+  auto launch = [&](const std::vector<GemmProb>& pr) {
+    return precision == BTA_PREC_TF32X3 ? gemm_launch_tc(pr, h->stream, h->ctl) : gemm_launch(pr, h->stream);
+  };
   size_t need = 8 * kAlign;
   int64_t maxn = 0;
   for (int k = 0; k < count; ++k) {
@@ -477,9 +488,9 @@ int bta_pobtasi_batched(bta_handle_t h, int count, const int64_t* n, const int64
       if (a[k] > 0) gemm_add(r, w[k].Ga, B_, Abi, B_, A_, -1.0, GF_A_T | GF_B_KN);
       pc.push_back(r);
     }
-    if (!pa.empty() && gemm_launch(pa, s)) return BTA_ERR_CUDA;
-    if (!pb.empty() && gemm_launch(pb, s)) return BTA_ERR_CUDA;
-    if (!pc.empty() && gemm_launch(pc, s)) return BTA_ERR_CUDA;
+    if (!pa.empty() && launch(pa)) return BTA_ERR_CUDA;
+    if (!pb.empty() && launch(pb)) return BTA_ERR_CUDA;
+    if (!pc.empty() && launch(pc)) return BTA_ERR_CUDA;
     for (int k = 0; k < count; ++k) {
       const int64_t i = n[k] - 1 - st;
       if (i < 0) continue;
@@ -494,6 +505,21 @@ int bta_pobtasi_batched(bta_handle_t h, int count, const int64_t* n, const int64
 int bta_pobtasi(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, double* L, double* Ab, double* T) {
   if (!h || n < 1 || b < 1 || a < 0 || !D || (n > 1 && !L) || (a > 0 && (!Ab || !T))) return BTA_ERR_INVALID;
   return bta_pobtasi_batched(h, 1, &n, &b, &a, &D, &L, &Ab, &T);
+}
+
+int bta_gemm(bta_handle_t h, int precision, int64_t M, int64_t N, int64_t K, double alpha, const double* A,
+             int64_t lda, int a_trans, const double* B, int64_t ldb, int b_kn, double beta, double* C, int64_t ldc,
+             int lower_only, int mirror) {
+  if (!h || M < 0 || N < 0 || K < 0 || M > INT32_MAX || N > INT32_MAX || K > INT32_MAX) return BTA_ERR_INVALID;
+  if (precision != BTA_PREC_FP64 && precision != BTA_PREC_TF32X3) return BTA_ERR_INVALID;
+  if (M == 0 || N == 0) return BTA_OK;
+  if (!C || ldc < N || (lower_only && M != N) || (mirror && !lower_only)) return BTA_ERR_INVALID;
+  if (K > 0 && (!A || !B || lda < (a_trans ? M : K) || ldb < (b_kn ? N : K))) return BTA_ERR_INVALID;
+  GemmProb p = gemm_prob(C, (int)ldc, (int)M, (int)N, beta, (lower_only ? GC_LOWER : 0) | (mirror ? GC_MIRROR : 0));
+  if (K > 0) gemm_add(p, A, (int)lda, B, (int)ldb, (int)K, alpha, (a_trans ? GF_A_T : 0) | (b_kn ? GF_B_KN : 0));
+  std::vector<GemmProb> v{p};
+  const int e = precision == BTA_PREC_TF32X3 ? gemm_launch_tc(v, h->stream, h->ctl) : gemm_launch(v, h->stream);
+  return e == 0 ? BTA_OK : BTA_ERR_CUDA;
 }
 
 int bta_logdet(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D, const double* T, int include_tip,

@@ -58,6 +58,11 @@ struct GemmBatch {
 // write overlapping C regions.  Returns a cudaError_t.
 int gemm_launch(const std::vector<GemmProb>& probs, cudaStream_t stream);
 
+// The same problems with FP32-class arithmetic on the tcgen05 tensor cores
+// (split TF32 x3, gemm_tc.cu).  abort_flag (device int) is raised when a
+// bounded wait inside the kernel gives up.
+int gemm_launch_tc(const std::vector<GemmProb>& probs, cudaStream_t stream, int* abort_flag);
+
 inline GemmProb gemm_prob(double* C, int ldc, int M, int N, double beta, int cflags = 0) {
   GemmProb p{};
   p.C = C;

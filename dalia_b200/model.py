@@ -113,6 +113,9 @@ def selinv_gemm_flops(n, b, a):
     return (n - 1) * (4 * b ** 3 + 6 * a * b ** 2) + n * (b ** 3 / 3 + 4 * a * b ** 2 + 4 * a * a * b)
 
 
+_PRECISIONS = {"fp64": _lib.BTA_PREC_FP64, "tf32x3": _lib.BTA_PREC_TF32X3}
+
+
 class BTAMatrix:
     """One BTA matrix in a single device allocation with D, L, Ab, T views."""
 
@@ -173,8 +176,21 @@ class SpatioTemporalModel:
     likelihood, evaluated on one GPU."""
 
     def __init__(self, prob, priors=None, fe_prec=1e-3, eps_gradient_f=1e-3, eps_inner_iteration=1e-3,
-                 inner_iteration_max_iter=50, device=None):
+                 inner_iteration_max_iter=50, device=None, selinv_precision="fp64", mixed_tolerance=1e-8):
+        """selinv_precision: arithmetic of the selected inversions behind the
+        adjoint gradient, "fp64" or "tf32x3" (FP32-class block products on the
+        tcgen05 tensor cores; factorisations, log-determinants and solves stay
+        FP64).  Every adjoint evaluation checks its selected inverses through
+        the identity <S, Q> = dim(Q) over the BTA pattern; a "tf32x3" point
+        whose relative residual exceeds mixed_tolerance is recomputed in FP64.
+        The residuals of the last evaluation are in ``last_check``."""
         import torch
+
+        if selinv_precision not in _PRECISIONS:
+            raise ValueError(f"selinv_precision must be one of {sorted(_PRECISIONS)}")
+        self.selinv_precision = selinv_precision
+        self.mixed_tol = float(mixed_tolerance)
+        self.last_check = []
 
         self.h = _lib.handle(device)
         self.device = self.h.device
@@ -276,6 +292,7 @@ class SpatioTemporalModel:
         self.nparts = 148
         self.part = torch.zeros(4096, **f64)
         self.dvec = torch.zeros(self.nobs, **f64)
+        self.ones_obs = torch.ones(self.nobs, **f64)
         self.slots = [self._new_slot(self.Qc, self.Qp)]
         # algorithmic flops of the factorisations / selected-inversion GEMMs
         # issued so far, and Newton steps taken (non-Gaussian likelihoods)
@@ -388,11 +405,11 @@ class SpatioTemporalModel:
         self._check(self.lib.bta_pobtaf_batched(self.h.bind_stream(), k, n, b, a, D, L, Ab, T, None),
                     "pobtaf_batched")
 
-    def selinv_batched(self, mats):
+    def selinv_batched(self, mats, precision="fp64"):
         self.work["selinv_gemm"] += sum(selinv_gemm_flops(m.n, m.b, m.a) for m in mats)
         k, n, b, a, D, L, Ab, T = self._batched_args(mats)
-        self._check(self.lib.bta_pobtasi_batched(self.h.bind_stream(), k, n, b, a, D, L, Ab, T),
-                    "pobtasi_batched")
+        self._check(self.lib.bta_pobtasi_batched_ex(self.h.bind_stream(), k, n, b, a, D, L, Ab, T,
+                                                    _PRECISIONS[precision]), "pobtasi_batched")
 
     def logdet_to(self, M: BTAMatrix, out):
         D, _, _, T = M.ptrs()
@@ -491,7 +508,35 @@ class SpatioTemporalModel:
         f, g = self.objective_adjoint_batched([theta])
         return f[0], g[0]
 
-    def objective_adjoint_batched(self, thetas):
+    def _identity_residuals(self, theta, Ic, Ip, rest_c, tip_c):
+        """Relative residuals of <S_c, Q_c> = N and <S_p, Q_st> = n b: the
+        spatio-temporal parts from the block inner products with the
+        Kronecker factors, rest_c = <S_c, A^T D A> and tip_c = <T(S_c), prior
+        tip>."""
+        mult = np.ones((2 * self.nt - 1, 1))
+        mult[self.nt:] = 2.0
+        cf = np.asarray(self.coef_blocks(theta), dtype=np.float64) * mult
+        nst = self.nt * self.ns
+        rc = abs(float(np.sum(cf * Ic)) + rest_c + tip_c - self.N) / self.N
+        rp = abs(float(np.sum(cf * Ip)) - nst) / nst
+        return rc, rp
+
+    def _mixed_fallback(self, thetas, fs, grads, precision):
+        """Recompute in FP64 the points whose selected-inverse check missed."""
+        if precision == "fp64":
+            return fs, grads
+        bad = [j for j, c in enumerate(self.last_check) if max(c["residual_c"], c["residual_p"]) > self.mixed_tol]
+        if not bad:
+            return fs, grads
+        checks = list(self.last_check)
+        f2, g2 = self.objective_adjoint_batched([thetas[j] for j in bad], precision="fp64")
+        for j, f, g, c in zip(bad, f2, g2, self.last_check):
+            fs[j], grads[j] = f, g
+            checks[j] = dict(c, fallback=True)
+        self.last_check = checks
+        return fs, grads
+
+    def objective_adjoint_batched(self, thetas, precision=None):
         """(f, exact gradient) at K theta points (e.g. the candidates of a line
         search), factorising and selected-inverting all 2K matrices (Q_c and
         Q_prior of every point) together:
@@ -500,8 +545,9 @@ class SpatioTemporalModel:
         with tr(S dQ_st) and mu^T dQ_st mu contracted block by block against
         the Kronecker factors (c0, g1, g2, g3) and S = Q^{-1} on the BTA
         pattern.  For a non-Gaussian likelihood see ``_adjoint_poisson_batched``."""
+        precision = self.selinv_precision if precision is None else precision
         if not self.gaussian:
-            return self._adjoint_poisson_batched(thetas)
+            return self._adjoint_poisson_batched(thetas, precision)
         thetas = [np.asarray(t, dtype=np.float64) for t in thetas]
         K = len(thetas)
         n, b, a = self.nt, self.ns, self.nb
@@ -530,7 +576,7 @@ class SpatioTemporalModel:
                                                 _lib.ptr(self.u_vals4), _lib.ptr(sl.x), _lib.ptr(sl.quad_st)),
                         "block_quad")
         # selected inverses and their contractions
-        self.selinv_batched([sl.Qc for sl in sls] + [sl.Qp for sl in sls])
+        self.selinv_batched([sl.Qc for sl in sls] + [sl.Qp for sl in sls], precision)
         for sl in sls:
             Dc, Lc, _, _ = sl.Qc.ptrs()
             Dp, Lp, _, _ = sl.Qp.ptrs()
@@ -544,6 +590,7 @@ class SpatioTemporalModel:
         mult = np.ones((2 * n - 1, 1))
         mult[n:] = 2.0  # each sub-diagonal block appears twice in the symmetric matrix
         fs, grads = [], []
+        self.last_check = []
         for sl, theta, tau in zip(sls, thetas, taus):
             s = sl.scal[:5].cpu().numpy()
             Ic = sl.inner_c.view(-1, 4).cpu().numpy()
@@ -560,9 +607,11 @@ class SpatioTemporalModel:
             grad[-1] = (0.5 * tau * tr_ata - s[1] + 0.5 * tau * s[3]
                         - (0.5 * self.nobs - 0.5 * tau * self.yty)
                         - self._dfun(self.log_prior_theta, theta, theta.size - 1))
+            rc, rp = self._identity_residuals(theta, Ic, Ip, tau * tr_ata, self.fe_prec * float(np.trace(Tsel)))
+            self.last_check.append({"precision": precision, "residual_c": rc, "residual_p": rp, "fallback": False})
             fs.append(float(f))
             grads.append(grad)
-        return fs, grads
+        return self._mixed_fallback(thetas, fs, grads, precision)
 
     # --------------------------------------------------------- marginals
     def _covariance(self, theta, x_star):
@@ -699,7 +748,7 @@ class SpatioTemporalModel:
         self._newton([sl], [theta])
         return self._f_poisson(sl, theta)
 
-    def _adjoint_poisson_batched(self, thetas):
+    def _adjoint_poisson_batched(self, thetas, precision="fp64"):
         """(f, gradient) at K theta points for the Poisson likelihood.
 
         With x* the mode, Q_c = Q_prior + A^T diag(d) A, d = e exp(A x*),
@@ -726,13 +775,14 @@ class SpatioTemporalModel:
             if sl.Sc is None:
                 sl.Sc = BTAMatrix(n, b, self.nb, self._dev)
             sl.Sc.buf.copy_(sl.Qc.buf)
-        self.selinv_batched([sl.Sc for sl in sls] + [sl.Qp for sl in sls])
+        self.selinv_batched([sl.Sc for sl in sls] + [sl.Qp for sl in sls], precision)
         for sl in sls:
             self._check(self.lib.bta_obs_quad(s, self.nobs, _lib.ptr(self.obs_off), _lib.ptr(self.obs_dst),
                                               _lib.ptr(self.obs_w), _lib.ptr(sl.Sc.buf), self.nb, _lib.ptr(self.X),
                                               _lib.ptr(sl.Sc.T) if self.nb else None, _lib.ptr(sl.dvec),
                                               _lib.ptr(sl.hvec)), "obs_quad")
             self.spmv(self.AT_rowptr, self.AT_col, self.AT_val, self.N, sl.hvec, sl.z)
+            self.dot_to(sl.hvec, self.ones_obs, sl.scal[7:8])  # <S_c, A^T diag(d) A>
         self.sweep_batched([sl.Qc for sl in sls], [sl.z for sl in sls], 0)
         self.sweep_batched([sl.Qc for sl in sls], [sl.z for sl in sls], 1)
         for sl in sls:
@@ -749,6 +799,7 @@ class SpatioTemporalModel:
         mult = np.ones((2 * n - 1, 1))
         mult[n:] = 2.0
         fs, grads = [], []
+        self.last_check = []
         for sl, theta in zip(sls, thetas):
             Ic = sl.inner_c.view(-1, 4).cpu().numpy()
             Ip = sl.inner_p.view(-1, 4).cpu().numpy()
@@ -759,6 +810,10 @@ class SpatioTemporalModel:
                 dc = self._dcoef(theta, k)
                 grad[k] = (0.5 * np.sum(dc * mult * (Ic - Ip + Qm)) + np.sum(dc * Bm)
                            - self._dfun(self.log_prior_theta, theta, k))
+            rest = float(sl.scal[7].item())
+            tip = self.fe_prec * float(torch.trace(sl.Sc.T).item()) if self.nb else 0.0
+            rc, rp = self._identity_residuals(theta, Ic, Ip, rest, tip)
+            self.last_check.append({"precision": precision, "residual_c": rc, "residual_p": rp, "fallback": False})
             fs.append(self._f_poisson(sl, theta))
             grads.append(grad)
-        return fs, grads
+        return self._mixed_fallback(thetas, fs, grads, precision)

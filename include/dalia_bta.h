@@ -77,6 +77,34 @@ int bta_pobtasi_batched(bta_handle_t h, int count, const int64_t* n, const int64
                         double* const* D, double* const* L, double* const* Ab, double* const* T);
 
 /*
+ * Arithmetic of the selected inversion's block products (no counterpart in
+ * the reference, which computes in the precision of its arrays):
+ * BTA_PREC_FP64 -- FP64 on the DMMA tensor pipe (the default everywhere);
+ * BTA_PREC_TF32X3 -- FP32-class: every FP64 operand is split into two TF32
+ * values and the products are accumulated in FP32 on the tcgen05 tensor
+ * cores (relative error of the selected inverse ~1e-7).  The factor, the
+ * diagonal-block inverses and all storage stay FP64.
+ */
+#define BTA_PREC_FP64 0
+#define BTA_PREC_TF32X3 1
+int bta_pobtasi_batched_ex(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                           double* const* D, double* const* L, double* const* Ab, double* const* T,
+                           int precision);
+
+/*
+ * C = beta C + alpha op(A) op(B) (row-major FP64; op(A)[m][k] = A[m*lda+k], or
+ * A[k*lda+m] with a_trans; op(B)[k][n] = B[n*ldb+k], or B[k*ldb+n] with b_kn)
+ * with the library's grouped GEMM in the given BTA_PREC_* arithmetic, on the
+ * handle's stream.  lower_only: compute and write only C[m][n] with m >= n
+ * (M == N); mirror (with lower_only): also write C[n][m].  The block-product
+ * kernel of the factorisation and selected inversion, exported for testing
+ * and for callers that need it; no counterpart in the reference.
+ */
+int bta_gemm(bta_handle_t h, int precision, int64_t M, int64_t N, int64_t K, double alpha, const double* A,
+             int64_t lda, int a_trans, const double* B, int64_t ldb, int b_kn, double beta, double* C, int64_t ldc,
+             int lower_only, int mirror);
+
+/*
  * One triangular sweep with the factor, in place on rhs (length n*b + a).
  * trans = 0: solve L y = rhs (Serinv trans="N"); trans = 1: solve L^T x = rhs
  * (trans="C").  Replaces pobtas (structured_solver.py:112-127) and, with a = 0,

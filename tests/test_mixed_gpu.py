@@ -1,0 +1,147 @@
+"""FP32-class (split TF32 x3, tcgen05 tensor cores) block products: the
+grouped GEMM through the C ABI against NumPy, the selected inversion against
+the FP64 oracle, and the adjoint gradient's accuracy check with its FP64
+fallback.
+
+Measured accuracy: the tensor cores accumulate in FP32 with truncating
+alignment, so the error grows with K (~1e-6 relative at K ~ 300 on random
+data, ~1e-5 for a selected inverse); the GEMM is held to 5e-6 and the
+selected inverse to 3e-5 (norm-wise).  That is not enough for the adjoint
+gradient's 1e-6 bar, so the default tolerance of the <S, Q> = N check
+sends TF32x3 points back to FP64, whose results must then be reproduced
+exactly."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from golden_util import load, problem, rel
+from oracle import bta_ref
+
+pytestmark = pytest.mark.gpu
+
+GEMM_CASES = [
+    # M, N, K, a_trans, b_kn, lower_only, mirror, alpha, beta
+    (128, 128, 32, 0, 0, 0, 0, 1.0, 0.0),
+    (200, 130, 70, 0, 0, 0, 0, -1.0, 1.0),
+    (257, 300, 129, 1, 0, 0, 0, 1.0, 0.0),
+    (300, 257, 200, 0, 1, 0, 0, 1.0, 1.0),
+    (190, 260, 333, 1, 1, 0, 0, -1.0, 0.0),
+    (6, 300, 301, 0, 1, 0, 0, 1.0, 0.0),
+    (300, 6, 300, 1, 0, 0, 0, 1.0, 0.0),
+    (310, 310, 150, 1, 1, 1, 1, 1.0, 0.0),
+    (384, 384, 512, 0, 0, 1, 0, -1.0, 1.0),
+    (100, 100, 0, 0, 0, 0, 0, 1.0, 0.5),
+]
+
+
+def _gemm(lib, h, prec, M, N, K, at, bkn, lower, mirror, alpha, beta, seed):
+    import torch
+
+    rng = np.random.default_rng(seed)
+    A = rng.standard_normal((K, M) if at else (M, K))
+    B = rng.standard_normal((K, N) if bkn else (N, K))
+    C = rng.standard_normal((M, N))
+    opA = A.T if at else A
+    opB = B if bkn else B.T
+    ref = beta * C + alpha * (opA @ opB)
+    dA, dB, dC = (torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (A, B, C))
+    from dalia_b200 import _lib
+
+    rc = lib.bta_gemm(h.bind_stream(), prec, M, N, K, alpha, _lib.ptr(dA), A.shape[1], at, _lib.ptr(dB),
+                      B.shape[1], bkn, beta, _lib.ptr(dC), N, lower, mirror)
+    _lib.check(rc, "gemm")
+    st = ctypes.c_int64(0)
+    _lib.check(lib.bta_get_status(h.bind_stream(), ctypes.byref(st)), "status")
+    got = dC.cpu().numpy()
+    if lower:
+        keep = np.tril(np.ones((M, N), dtype=bool))
+        if mirror:
+            keep = keep | keep.T
+            ref = np.where(np.tril(np.ones((M, N), dtype=bool)), ref, ref.T)
+        exp = np.where(keep, ref, C)
+    else:
+        exp = ref
+    return got, exp
+
+
+@pytest.mark.parametrize("case", GEMM_CASES)
+def test_gemm_tf32x3_and_fp64_match_numpy(case):
+    from dalia_b200 import _lib
+
+    lib = _lib.load()
+    h = _lib.handle()
+    M, N, K, at, bkn, lower, mirror, alpha, beta = case
+    got, exp = _gemm(lib, h, _lib.BTA_PREC_FP64, *case, seed=M + N + K)
+    assert rel(got, exp) < 1e-13
+    got, exp = _gemm(lib, h, _lib.BTA_PREC_TF32X3, *case, seed=M + N + K)
+    assert rel(got, exp) < 5e-6
+
+
+@pytest.mark.parametrize("n,b,a", [(3, 200, 6), (4, 129, 0), (2, 300, 70)])
+def test_selinv_tf32x3_matches_oracle(n, b, a):
+    import torch
+
+    from dalia_b200 import _lib
+
+    lib = _lib.load()
+    h = _lib.handle()
+    rng = np.random.default_rng(7 * n + b + a)
+    D, L, Ab, T = bta_ref.random_bta(n, b, a, rng)
+    ref = [x.copy() for x in (D, L, Ab, T)]
+    bta_ref.pobtaf(*ref)
+    bta_ref.pobtasi(*ref)
+    d = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (D, L, Ab, T)]
+    arr = lambda t: (ctypes.c_void_p * 1)(t.data_ptr() if t.numel() else None)
+    i64 = lambda v: (ctypes.c_int64 * 1)(v)
+    args = (h.bind_stream(), 1, i64(n), i64(b), i64(a), arr(d[0]), arr(d[1]), arr(d[2]), arr(d[3]))
+    _lib.check(lib.bta_pobtaf_batched(*args, None), "pobtaf")
+    _lib.check(lib.bta_pobtasi_batched_ex(*args, _lib.BTA_PREC_TF32X3), "pobtasi")
+    st = ctypes.c_int64(0)
+    _lib.check(lib.bta_get_status(h.bind_stream(), ctypes.byref(st)), "status")
+    got = [t.cpu().numpy() for t in d]
+    assert rel(got[0], ref[0]) < 3e-5
+    if n > 1:
+        assert rel(got[1], ref[1]) < 3e-5
+    if a:
+        assert rel(got[2], ref[2]) < 3e-5 and rel(got[3], ref[3]) < 3e-5
+
+
+@pytest.mark.parametrize("name", ["gst_300x10", "pst_150x6"])
+def test_tf32x3_adjoint_check_and_fallback(name):
+    from dalia_b200.model import SpatioTemporalModel
+
+    g = load(name)
+    prob = problem(g)
+    th = g["theta"]
+    m64 = SpatioTemporalModel(prob)
+    f64, g64 = m64.objective_adjoint(th)
+    chk64 = m64.last_check[0]
+    assert chk64["residual_c"] < 1e-11 and chk64["residual_p"] < 1e-11
+    # no fallback: the check reports the reduced precision
+    mm = SpatioTemporalModel(prob, selinv_precision="tf32x3", mixed_tolerance=1.0)
+    fm, gm = mm.objective_adjoint(th)
+    chk = mm.last_check[0]
+    assert chk["precision"] == "tf32x3" and not chk["fallback"]
+    assert abs(fm - f64) < 1e-12 * abs(f64)
+    assert rel(gm, g64) < 1e-2
+    assert max(chk["residual_c"], chk["residual_p"]) > 100 * max(chk64["residual_c"], chk64["residual_p"])
+    # default tolerance: the point is recomputed in FP64
+    md = SpatioTemporalModel(prob, selinv_precision="tf32x3")
+    fd, gd = md.objective_adjoint(th)
+    assert md.last_check[0]["fallback"]
+    assert abs(fd - f64) < 1e-12 * abs(f64) and rel(gd, g64) < 1e-10
+
+
+def test_mixed_fallback_recomputes_in_fp64():
+    from dalia_b200.model import SpatioTemporalModel
+
+    g = load("gst_ragged")
+    prob = problem(g)
+    th = g["theta"]
+    f64, g64 = SpatioTemporalModel(prob).objective_adjoint(th)
+    mm = SpatioTemporalModel(prob, selinv_precision="tf32x3", mixed_tolerance=0.0)
+    fm, gm = mm.objective_adjoint(th)
+    assert mm.last_check[0]["fallback"]
+    assert abs(fm - f64) < 1e-12 * abs(f64)
+    assert rel(gm, g64) < 1e-10
