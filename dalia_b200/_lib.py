@@ -74,6 +74,12 @@ SIGNATURES = {
                                _c_void_p]),
     "bta_block_quad": (_int, [_c_void_p, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p]),
     "bta_gather_dot": (_int, [_c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _int, _c_void_p]),
+    "bta_assemble_prior_mv": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                     _c_void_p, _c_void_p]),
+    "bta_block_inner_mv": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                  _c_void_p, _c_void_p]),
+    "bta_block_quad_mv": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                 _c_void_p]),
     "bta_kron_symv": (_int, [_c_void_p, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _dbl,
                              _dbl, _c_void_p]),
     "bta_poisson_terms": (_int, [_c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,

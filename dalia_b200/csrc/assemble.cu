@@ -17,21 +17,24 @@
 
 namespace {
 
-// one CTA per (block, 8-row slab): write rows of D_t (blk < n) or L_t (blk >= n)
-__global__ void __launch_bounds__(256) assemble_prior_kernel(int n, int b, const double* coef, const int* rowptr,
-                                                             const int* colidx, const double* vals4, double* D,
-                                                             double* L) {
+// One CTA per (block, 8-row slab): write rows of D_t (blk < n) or L_t
+// (blk >= n).  With nv variates interleaved per time step the block is
+// (nv ns) x (nv ns); row r = v ns + s holds, for every variate w, the spatial
+// row s of sub-block (v, w) = sum_K coef[blk][v][w][K] K at columns w ns + c.
+__global__ void __launch_bounds__(256) assemble_prior_kernel(int n, int ns, int nv, const double* coef,
+                                                             const int* rowptr, const int* colidx,
+                                                             const double* vals4, double* D, double* L) {
   const int rows_per = 8;
+  const int b = nv * ns;
   const int slabs = (b + rows_per - 1) / rows_per;
   const int blk = blockIdx.x / slabs, slab = blockIdx.x % slabs;
   const bool lower = blk >= n;
   const int t = lower ? blk - n : blk;
   double* M = lower ? L + (size_t)t * b * b : D + (size_t)t * b * b;
-  const double* cf = coef + (size_t)blk * 4;
-  const double c0 = cf[0], c1 = cf[1], c2 = cf[2], c3 = cf[3];
   for (int rr = 0; rr < rows_per; ++rr) {
     const int row = slab * rows_per + rr;
     if (row >= b) break;
+    const int v = row / ns, sr = row - v * ns;
     double* out = M + (size_t)row * b;
     // zero the row (vectorised when aligned)
     if ((b & 1) == 0 && ((reinterpret_cast<uintptr_t>(out) & 15) == 0)) {
@@ -41,9 +44,12 @@ __global__ void __launch_bounds__(256) assemble_prior_kernel(int n, int b, const
       for (int c = threadIdx.x; c < b; c += blockDim.x) out[c] = 0.0;
     }
     __syncthreads();
-    for (int e = rowptr[row] + threadIdx.x; e < rowptr[row + 1]; e += blockDim.x) {
-      const double* v = vals4 + (size_t)e * 4;
-      out[colidx[e]] = c0 * v[0] + c1 * v[1] + c2 * v[2] + c3 * v[3];
+    const int e0 = rowptr[sr], e1 = rowptr[sr + 1], len = e1 - e0;
+    for (int q = threadIdx.x; q < nv * len; q += blockDim.x) {
+      const int w = q / len, e = e0 + (q - w * len);
+      const double* cf = coef + (((size_t)blk * nv + v) * nv + w) * 4;
+      const double* vv = vals4 + (size_t)e * 4;
+      out[w * ns + colidx[e]] = cf[0] * vv[0] + cf[1] * vv[1] + cf[2] * vv[2] + cf[3] * vv[3];
     }
     __syncthreads();
   }
@@ -103,30 +109,29 @@ __global__ void tip_final_kernel(int nparts, int a, const double* part, double p
   }
 }
 
-// out[blk][K] = sum over the union pattern of block blk of S_blk[row][col] * K_e
-// (blk < n: diagonal block D_t; else sub-diagonal block L_{blk-n}).
-__global__ void __launch_bounds__(256) block_inner_kernel(int n, int b, const int* rowptr, const int* colidx,
-                                                          const double* vals4, const double* D, const double* L,
-                                                          double* out) {
+// out[blk][v][w][K] = sum over the union pattern of sub-block (v, w) of block
+// blk of S[v ns + s][w ns + c] * K[s][c] (blk < n: diagonal block D_t; else
+// sub-diagonal block L_{blk-n}).  One CTA per (blk, v, w).
+__global__ void __launch_bounds__(256) block_inner_kernel(int n, int ns, int nv, const int* rowptr,
+                                                          const int* colidx, const double* vals4, const double* D,
+                                                          const double* L, double* out) {
   __shared__ double red[4][256];
-  const int blk = blockIdx.x;
+  const int blk = blockIdx.x / (nv * nv), vw = blockIdx.x % (nv * nv), v = vw / nv, w = vw % nv;
+  const int b = nv * ns;
   const bool lower = blk >= n;
   const int t = lower ? blk - n : blk;
-  const double* M = lower ? L + (size_t)t * b * b : D + (size_t)t * b * b;
+  const double* M = (lower ? L + (size_t)t * b * b : D + (size_t)t * b * b) + (size_t)v * ns * b + w * ns;
   double s[4] = {0.0, 0.0, 0.0, 0.0};
-  const int nnz = rowptr[b];
-  // row of entry e by binary search is avoided: walk rows with a strided loop
-  for (int row = threadIdx.x; row < b; row += blockDim.x) {
+  for (int row = threadIdx.x; row < ns; row += blockDim.x) {
     for (int e = rowptr[row]; e < rowptr[row + 1]; ++e) {
       const double m = M[(size_t)row * b + colidx[e]];
-      const double* v = vals4 + (size_t)e * 4;
-      s[0] += m * v[0];
-      s[1] += m * v[1];
-      s[2] += m * v[2];
-      s[3] += m * v[3];
+      const double* vv = vals4 + (size_t)e * 4;
+      s[0] += m * vv[0];
+      s[1] += m * vv[1];
+      s[2] += m * vv[2];
+      s[3] += m * vv[3];
     }
   }
-  (void)nnz;
   for (int k = 0; k < 4; ++k) red[k][threadIdx.x] = s[k];
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
@@ -134,29 +139,32 @@ __global__ void __launch_bounds__(256) block_inner_kernel(int n, int b, const in
       for (int k = 0; k < 4; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + o];
     __syncthreads();
   }
-  if (threadIdx.x < 4) out[(size_t)blk * 4 + threadIdx.x] = red[threadIdx.x][0];
+  if (threadIdx.x < 4) out[(size_t)blockIdx.x * 4 + threadIdx.x] = red[threadIdx.x][0];
 }
 
-// out[blk][K] = x_r^T K x_c over the union pattern, (r, c) = (t, t) for the
-// diagonal block t = blk < n, (t+1, t) for the sub-diagonal block t = blk-n.
-__global__ void __launch_bounds__(256) block_quad_kernel(int n, int b, const int* rowptr, const int* colidx,
-                                                         const double* vals4, const double* x, double* out) {
+// out[blk][v][w][K] = x_{r,v}^T K x_{c,w} over the union pattern, where x_{t,v}
+// is variate v's segment of time step t, (r, c) = (t, t) for the diagonal
+// block t = blk < n and (t+1, t) for the sub-diagonal block t = blk - n.
+__global__ void __launch_bounds__(256) block_quad_kernel(int n, int ns, int nv, const int* rowptr,
+                                                         const int* colidx, const double* vals4, const double* x,
+                                                         double* out) {
   __shared__ double red[4][256];
-  const int blk = blockIdx.x;
+  const int blk = blockIdx.x / (nv * nv), vw = blockIdx.x % (nv * nv), v = vw / nv, w = vw % nv;
+  const int b = nv * ns;
   const bool lower = blk >= n;
   const int t = lower ? blk - n : blk;
-  const double* xr = x + (size_t)(lower ? t + 1 : t) * b;
-  const double* xc = x + (size_t)t * b;
+  const double* xr = x + (size_t)(lower ? t + 1 : t) * b + v * ns;
+  const double* xc = x + (size_t)t * b + w * ns;
   double s[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int row = threadIdx.x; row < b; row += blockDim.x) {
+  for (int row = threadIdx.x; row < ns; row += blockDim.x) {
     const double xv = xr[row];
     for (int e = rowptr[row]; e < rowptr[row + 1]; ++e) {
       const double m = xv * xc[colidx[e]];
-      const double* v = vals4 + (size_t)e * 4;
-      s[0] += m * v[0];
-      s[1] += m * v[1];
-      s[2] += m * v[2];
-      s[3] += m * v[3];
+      const double* vv = vals4 + (size_t)e * 4;
+      s[0] += m * vv[0];
+      s[1] += m * vv[1];
+      s[2] += m * vv[2];
+      s[3] += m * vv[3];
     }
   }
   for (int k = 0; k < 4; ++k) red[k][threadIdx.x] = s[k];
@@ -166,7 +174,7 @@ __global__ void __launch_bounds__(256) block_quad_kernel(int n, int b, const int
       for (int k = 0; k < 4; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + o];
     __syncthreads();
   }
-  if (threadIdx.x < 4) out[(size_t)blk * 4 + threadIdx.x] = red[threadIdx.x][0];
+  if (threadIdx.x < 4) out[(size_t)blockIdx.x * 4 + threadIdx.x] = red[threadIdx.x][0];
 }
 
 // out[blockIdx] partial of sum_e w[e] * base[idx[e]]
@@ -412,17 +420,24 @@ int bta_axpby(void* stream, int64_t n, double alpha, const double* x, double bet
 }
 
 
-int bta_assemble_prior(void* stream, int64_t n, int64_t b, const double* coef, const int* rowptr, const int* colidx,
-                       const double* vals4, double* D, double* L) {
-  if (n < 1 || b < 1 || !coef || !rowptr || !colidx || !vals4 || !D || (n > 1 && !L)) return BTA_ERR_INVALID;
+int bta_assemble_prior_mv(void* stream, int64_t n, int64_t ns, int64_t nv, const double* coef, const int* rowptr,
+                          const int* colidx, const double* vals4, double* D, double* L) {
+  if (n < 1 || ns < 1 || nv < 1 || !coef || !rowptr || !colidx || !vals4 || !D || (n > 1 && !L))
+    return BTA_ERR_INVALID;
+  const int64_t b = nv * ns;
   const int slabs = (int)((b + 7) / 8);
   const int nblk = (int)(2 * n - 1);
   {
     bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
-    assemble_prior_kernel<<<nblk * slabs, 256, 0, (cudaStream_t)stream>>>((int)n, (int)b, coef, rowptr, colidx, vals4,
-                                                                         D, L);
+    assemble_prior_kernel<<<nblk * slabs, 256, 0, (cudaStream_t)stream>>>((int)n, (int)ns, (int)nv, coef, rowptr,
+                                                                         colidx, vals4, D, L);
   }
   return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
+}
+
+int bta_assemble_prior(void* stream, int64_t n, int64_t b, const double* coef, const int* rowptr, const int* colidx,
+                       const double* vals4, double* D, double* L) {
+  return bta_assemble_prior_mv(stream, n, b, 1, coef, rowptr, colidx, vals4, D, L);
 }
 
 int bta_add_entries(void* stream, int64_t nent, const int64_t* dst, const int64_t* off, const int* obs,
@@ -451,25 +466,36 @@ int bta_arrow_tip(void* stream, int64_t nobs, int64_t a, const double* X, const 
   return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
 }
 
-int bta_block_inner(void* stream, int64_t n, int64_t b, const int* rowptr, const int* colidx, const double* vals4,
-                    const double* D, const double* L, double* out) {
-  if (n < 1 || b < 1 || !out) return BTA_ERR_INVALID;
+int bta_block_inner_mv(void* stream, int64_t n, int64_t ns, int64_t nv, const int* rowptr, const int* colidx,
+                       const double* vals4, const double* D, const double* L, double* out) {
+  if (n < 1 || ns < 1 || nv < 1 || !out || !D || (n > 1 && !L)) return BTA_ERR_INVALID;
   {
     bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
-    block_inner_kernel<<<(int)(2 * n - 1), 256, 0, (cudaStream_t)stream>>>((int)n, (int)b, rowptr, colidx, vals4, D, L,
-                                                                         out);
+    block_inner_kernel<<<(int)((2 * n - 1) * nv * nv), 256, 0, (cudaStream_t)stream>>>(
+        (int)n, (int)ns, (int)nv, rowptr, colidx, vals4, D, L, out);
+  }
+  return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
+}
+
+int bta_block_inner(void* stream, int64_t n, int64_t b, const int* rowptr, const int* colidx, const double* vals4,
+                    const double* D, const double* L, double* out) {
+  return bta_block_inner_mv(stream, n, b, 1, rowptr, colidx, vals4, D, L, out);
+}
+
+int bta_block_quad_mv(void* stream, int64_t n, int64_t ns, int64_t nv, const int* rowptr, const int* colidx,
+                      const double* vals4, const double* x, double* out) {
+  if (n < 1 || ns < 1 || nv < 1 || !out || !x) return BTA_ERR_INVALID;
+  {
+    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
+    block_quad_kernel<<<(int)((2 * n - 1) * nv * nv), 256, 0, (cudaStream_t)stream>>>(
+        (int)n, (int)ns, (int)nv, rowptr, colidx, vals4, x, out);
   }
   return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
 }
 
 int bta_block_quad(void* stream, int64_t n, int64_t b, const int* rowptr, const int* colidx, const double* vals4,
                    const double* x, double* out) {
-  if (n < 1 || b < 1 || !out || !x) return BTA_ERR_INVALID;
-  {
-    bta::ProfScope _ps(bta::PROF_OTHER, (cudaStream_t)stream);
-    block_quad_kernel<<<(int)(2 * n - 1), 256, 0, (cudaStream_t)stream>>>((int)n, (int)b, rowptr, colidx, vals4, x, out);
-  }
-  return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
+  return bta_block_quad_mv(stream, n, b, 1, rowptr, colidx, vals4, x, out);
 }
 
 int bta_gather_dot(void* stream, int64_t nent, const int64_t* idx, const double* w, const double* base, double* part,

@@ -143,7 +143,7 @@ class _Slot:
     """Device state of one theta point: the two BTA matrices, vectors and
     read-back scalars (one per point of a batched evaluation)."""
 
-    def __init__(self, n, b, a, N, nobs, device, Qc=None, Qp=None):
+    def __init__(self, n, b, a, N, nobs, device, Qc=None, Qp=None, nv=1):
         import torch
 
         f64 = dict(dtype=torch.float64, device=device)
@@ -153,7 +153,8 @@ class _Slot:
         self.x = torch.zeros(N, **f64)  # latent mean / mode, like the reference's model.x
         self.eta = torch.zeros(nobs, **f64)
         self.scal = torch.zeros(16, **f64)
-        nb4 = (2 * n - 1) * 4
+        nb4 = (2 * n - 1) * 4 * nv * nv  # [block][v][w][K]
+        self.vscal = torch.zeros(3 * nv, **f64)  # per variate: tr(S A_v^T A_v), |A_v mu|^2, (A_v mu)^T y_v
         self.inner_c = torch.zeros(nb4, **f64)
         self.inner_p = torch.zeros(nb4, **f64)
         self.quad_st = torch.zeros(nb4, **f64)
@@ -197,9 +198,14 @@ class SpatioTemporalModel:
         self.lib = _lib.load()
         dev = self.device
         self.ns, self.nt, self.nb = int(prob.ns), int(prob.nt), int(prob.nb)
-        n, b, a = self.nt, self.ns, self.nb
+        # nv variates interleaved per time step (1: univariate): block size nv ns
+        self.nv = int(getattr(prob, "nv", 1))
+        self.b = self.nv * self.ns
+        n, b, a, ns = self.nt, self.b, self.nb, self.ns
         self.N = n * b + a
         self.gaussian = prob.likelihood == "gaussian"
+        if self.nv > 1 and not self.gaussian:
+            raise NotImplementedError("multivariate models: Gaussian likelihoods only")
         self.priors = dict(DEFAULT_PRIORS if priors is None else priors)
         self.theta_keys = ["r_s", "r_t", "sigma_st"] + (["prec_o"] if self.gaussian else [])
         self.fe_prec = float(fe_prec)
@@ -210,7 +216,7 @@ class SpatioTemporalModel:
         # --- union pattern of c0, g1, g2, g3 with four values per entry
         U = (abs(prob.c0) + abs(prob.g1) + abs(prob.g2) + abs(prob.g3)).tocsr()
         U.sort_indices()
-        rows = np.repeat(np.arange(b), np.diff(U.indptr))
+        rows = np.repeat(np.arange(ns), np.diff(U.indptr))
         cols = U.indices
         vals4 = np.stack([np.asarray(sps.csr_matrix(K)[rows, cols]).ravel()
                           for K in (prob.c0, prob.g1, prob.g2, prob.g3)], axis=1)
@@ -242,9 +248,19 @@ class SpatioTemporalModel:
         self.e = torch.tensor(self.e_host, **f64)
         X = A[:, n * b:].toarray() if a > 0 else np.zeros((self.nobs, 0))
         self.X = torch.tensor(np.ascontiguousarray(X), **f64)
-        self.XtX_host = X.T @ X
-        self.yty = float(self.y_host @ self.y_host)
-        self.Aty = torch.tensor(A.T @ self.y_host, **f64)
+        # observation ranges of the variates, and the theta index of each
+        # variate's Gaussian precision
+        self.var_ranges = list(getattr(prob, "var_ranges", [(0, self.nobs)]))
+        self.tau_idx = list(getattr(prob, "tau_idx", [len(self.theta_keys) - 1] if self.gaussian else []))
+        self.XtX_var = [X[lo:hi].T @ X[lo:hi] for lo, hi in self.var_ranges]
+        self.yty_var = [float(self.y_host[lo:hi] @ self.y_host[lo:hi]) for lo, hi in self.var_ranges]
+        self.nobs_var = [hi - lo for lo, hi in self.var_ranges]
+        Aty = []
+        for lo, hi in self.var_ranges:
+            yv = np.zeros(self.nobs)
+            yv[lo:hi] = self.y_host[lo:hi]
+            Aty.append(torch.tensor(A.T @ yv, **f64))
+        self.Aty_var = Aty
 
         # --- A^T D A entry lists on the BTA pattern (tip handled separately)
         self.Qc = BTAMatrix(n, b, a, dev)
@@ -284,9 +300,13 @@ class SpatioTemporalModel:
         self.ent_obs = torch.tensor(obs.astype(np.int32), **i32)
         self.ent_fac = torch.tensor(fac, **f64)
         self.nent = int(ud.size)
-        # trace weights of A^T A on the stored entries (lower blocks count twice)
-        sumfac = np.add.reduceat(fac, start) if fac.size else np.zeros(0)
-        self.ata_w = torch.tensor(sumfac * kindmult[start], **f64)
+        # trace weights of A_v^T A_v on the stored entries, per variate (lower
+        # blocks count twice)
+        self.ata_w_var = []
+        for lo, hi in self.var_ranges:
+            fv = np.where((obs >= lo) & (obs < hi), fac, 0.0)
+            sumfac = np.add.reduceat(fv, start) if fv.size else np.zeros(0)
+            self.ata_w_var.append(torch.tensor(sumfac * kindmult[start], **f64))
 
         # --- scratch
         self.nparts = 148
@@ -299,7 +319,7 @@ class SpatioTemporalModel:
         self.work = {"factor": 0.0, "selinv_gemm": 0.0, "newton_steps": 0}
 
     def _new_slot(self, Qc=None, Qp=None):
-        return _Slot(self.nt, self.ns, self.nb, self.N, self.nobs, self._dev, Qc, Qp)
+        return _Slot(self.nt, self.b, self.nb, self.N, self.nobs, self._dev, Qc, Qp, self.nv)
 
     def slot(self, j):
         while len(self.slots) <= j:
@@ -317,7 +337,11 @@ class SpatioTemporalModel:
         """Coefficients of (c0, g1, g2, g3) for every lower BTA block of Q_st;
         rows 0..n-1 diagonal blocks, rows n..2n-2 sub-diagonal blocks.
         Complex-safe."""
-        g_s, g_t, g_st = theta_to_gamma(theta[0], theta[1], theta[2])
+        return self._coef_field(theta[0], theta[1], theta[2])
+
+    def _coef_field(self, r_s, r_t, sigma_st):
+        """Kronecker coefficients of one DEMF(1,2,1) field, (2n-1) x 4."""
+        g_s, g_t, g_st = theta_to_gamma(r_s, r_t, sigma_st)
         k2 = np.exp(2 * g_s)
         E = np.exp(2 * g_st)
         u = np.exp(g_t)
@@ -339,8 +363,31 @@ class SpatioTemporalModel:
         return s
 
     def lik0(self, theta):
-        """Gaussian log-likelihood at eta = 0 (``gaussian.py:55-62``)."""
-        return 0.5 * theta[-1] * self.nobs - 0.5 * np.exp(theta[-1]) * self.yty
+        """Gaussian log-likelihood at eta = 0 (``gaussian.py:55-62``), summed
+        over the variates."""
+        s = 0.0
+        for k, nv_obs, yty in zip(self.tau_idx, self.nobs_var, self.yty_var):
+            s = s + 0.5 * theta[k] * nv_obs - 0.5 * np.exp(theta[k]) * yty
+        return s
+
+    def _gauss_conditional(self, theta, sl):
+        """Q_c of a Gaussian likelihood: one precision scales A^T A, several
+        (one per variate) fill sl.dvec observation range by range."""
+        if len(self.tau_idx) == 1:
+            self.assemble_conditional(theta, None, math.exp(theta[self.tau_idx[0]]), sl)
+            return
+        s = self._stream()
+        for k, (lo, hi) in zip(self.tau_idx, self.var_ranges):
+            self._check(self.lib.bta_axpby(s, hi - lo, math.exp(theta[k]), _lib.ptr(self.ones_obs[lo:hi]), 0.0,
+                                           _lib.ptr(sl.dvec[lo:hi])), "axpby")
+        self.assemble_conditional(theta, sl.dvec, 1.0, sl)
+
+    def _gauss_rhs(self, theta, sl):
+        """Information vector at x = 0, eta = 0: sum_v tau_v A_v^T y_v."""
+        s = self._stream()
+        for j, k in enumerate(self.tau_idx):
+            self._check(self.lib.bta_axpby(s, self.N, math.exp(theta[k]), _lib.ptr(self.Aty_var[j]),
+                                           1.0 if j else 0.0, _lib.ptr(sl.rhs)), "axpby")
 
     # ---------------------------------------------------------------- device
     def _stream(self):
@@ -354,9 +401,9 @@ class SpatioTemporalModel:
         sl.coef_host[which].numpy()[:] = c
         sl.coef_dev[which].copy_(sl.coef_host[which], non_blocking=True)
         D, L, _, _ = M.ptrs()
-        self._check(self.lib.bta_assemble_prior(self._stream(), M.n, M.b, _lib.ptr(sl.coef_dev[which]),
-                                                _lib.ptr(self.u_rowptr), _lib.ptr(self.u_col),
-                                                _lib.ptr(self.u_vals4), D, L), "assemble_prior")
+        self._check(self.lib.bta_assemble_prior_mv(self._stream(), M.n, self.ns, self.nv, _lib.ptr(sl.coef_dev[which]),
+                                                   _lib.ptr(self.u_rowptr), _lib.ptr(self.u_col),
+                                                   _lib.ptr(self.u_vals4), D, L), "assemble_prior")
 
     def assemble_conditional(self, theta, d=None, dscale=1.0, sl=None):
         """Q_c = Q_prior + A^T diag(dscale * d) A in BTA storage (``model.py:384-423``);
@@ -454,13 +501,11 @@ class SpatioTemporalModel:
         _lib.check(self.lib.bta_reset_status(self.h.bind_stream()), "reset")
         if self.gaussian:
             sl = self.slots[0]
-            tau = math.exp(theta[-1])
-            self.assemble_conditional(theta, None, tau, sl)
+            self._gauss_conditional(theta, sl)
             self.factor(sl.Qc)
             self.logdet_to(sl.Qc, sl.scal[0:1])
-            # rhs = -Q_prior x + A^T grad(lik) at x = 0, eta = 0  ->  tau A^T y
-            self._check(self.lib.bta_axpby(self._stream(), self.N, tau, _lib.ptr(self.Aty), 0.0,
-                                           _lib.ptr(sl.rhs)), "axpby")
+            # rhs = -Q_prior x + A^T grad(lik) at x = 0, eta = 0  ->  sum_v tau_v A_v^T y_v
+            self._gauss_rhs(theta, sl)
             sl.x.copy_(sl.rhs)
             self.sweep(sl.Qc, sl.x, 0)
             self.sweep(sl.Qc, sl.x, 1)
@@ -516,7 +561,7 @@ class SpatioTemporalModel:
         mult = np.ones((2 * self.nt - 1, 1))
         mult[self.nt:] = 2.0
         cf = np.asarray(self.coef_blocks(theta), dtype=np.float64) * mult
-        nst = self.nt * self.ns
+        nst = self.nt * self.b
         rc = abs(float(np.sum(cf * Ic)) + rest_c + tip_c - self.N) / self.N
         rp = abs(float(np.sum(cf * Ip)) - nst) / nst
         return rc, rp
@@ -550,30 +595,31 @@ class SpatioTemporalModel:
             return self._adjoint_poisson_batched(thetas, precision)
         thetas = [np.asarray(t, dtype=np.float64) for t in thetas]
         K = len(thetas)
-        n, b, a = self.nt, self.ns, self.nb
+        n, a, ns, nv = self.nt, self.nb, self.ns, self.nv
         stream = self._stream()
         sls = [self.slot(j) for j in range(K)]
-        taus = [math.exp(t[-1]) for t in thetas]
+        pat = (_lib.ptr(self.u_rowptr), _lib.ptr(self.u_col), _lib.ptr(self.u_vals4))
         _lib.check(self.lib.bta_reset_status(self.h.bind_stream()), "reset")
-        for sl, th, tau in zip(sls, thetas, taus):
-            self.assemble_conditional(th, None, tau, sl)
+        for sl, th in zip(sls, thetas):
+            self._gauss_conditional(th, sl)
             self.assemble_prior_bt(th, sl)
         self.factor_batched([sl.Qc for sl in sls] + [sl.Qp for sl in sls])
-        for sl, tau in zip(sls, taus):
+        for sl, th in zip(sls, thetas):
             self.logdet_to(sl.Qc, sl.scal[0:1])
             self.logdet_to(sl.Qp, sl.scal[2:3])
-            self._check(self.lib.bta_axpby(stream, self.N, tau, _lib.ptr(self.Aty), 0.0, _lib.ptr(sl.rhs)), "axpby")
+            self._gauss_rhs(th, sl)
             sl.x.copy_(sl.rhs)
         self.sweep_batched([sl.Qc for sl in sls], [sl.x for sl in sls], 0)
         for sl in sls:
             self.dot_to(sl.x, sl.x, sl.scal[1:2])  # b^T Q^-1 b = |L^-1 b|^2
         self.sweep_batched([sl.Qc for sl in sls], [sl.x for sl in sls], 1)  # mu
         for sl in sls:
-            # |A mu|^2 and mu^T (E_tt' (x) K) mu
+            # per variate |A_v mu|^2 and (A_v mu)^T y_v; mu^T (E_tt' (x) K) mu per sub-block
             self.spmv(self.A_rowptr, self.A_col, self.A_val, self.nobs, sl.x, sl.eta)
-            self.dot_to(sl.eta, sl.eta, sl.scal[3:4])
-            self._check(self.lib.bta_block_quad(stream, n, b, _lib.ptr(self.u_rowptr), _lib.ptr(self.u_col),
-                                                _lib.ptr(self.u_vals4), _lib.ptr(sl.x), _lib.ptr(sl.quad_st)),
+            for j, (lo, hi) in enumerate(self.var_ranges):
+                self.dot_to(sl.eta[lo:hi], sl.eta[lo:hi], sl.vscal[3 * j + 1:3 * j + 2])
+                self.dot_to(sl.eta[lo:hi], self.y[lo:hi], sl.vscal[3 * j + 2:3 * j + 3])
+            self._check(self.lib.bta_block_quad_mv(stream, n, ns, nv, *pat, _lib.ptr(sl.x), _lib.ptr(sl.quad_st)),
                         "block_quad")
         # selected inverses and their contractions
         self.selinv_batched([sl.Qc for sl in sls] + [sl.Qp for sl in sls], precision)
@@ -581,33 +627,39 @@ class SpatioTemporalModel:
             Dc, Lc, _, _ = sl.Qc.ptrs()
             Dp, Lp, _, _ = sl.Qp.ptrs()
             for (Dm, Lm, out) in ((Dc, Lc, sl.inner_c), (Dp, Lp, sl.inner_p)):
-                self._check(self.lib.bta_block_inner(stream, n, b, _lib.ptr(self.u_rowptr), _lib.ptr(self.u_col),
-                                                     _lib.ptr(self.u_vals4), Dm, Lm, _lib.ptr(out)), "block_inner")
-            self._check(self.lib.bta_gather_dot(stream, self.nent, _lib.ptr(self.ent_dst), _lib.ptr(self.ata_w),
-                                                _lib.ptr(sl.Qc.buf), _lib.ptr(self.part), self.nparts,
-                                                _lib.ptr(sl.scal[4:5])), "gather_dot")
+                self._check(self.lib.bta_block_inner_mv(stream, n, ns, nv, *pat, Dm, Lm, _lib.ptr(out)), "block_inner")
+            for j in range(len(self.var_ranges)):
+                self._check(self.lib.bta_gather_dot(stream, self.nent, _lib.ptr(self.ent_dst),
+                                                    _lib.ptr(self.ata_w_var[j]), _lib.ptr(sl.Qc.buf),
+                                                    _lib.ptr(self.part), self.nparts,
+                                                    _lib.ptr(sl.vscal[3 * j:3 * j + 1])), "gather_dot")
         self.status()
         mult = np.ones((2 * n - 1, 1))
         mult[n:] = 2.0  # each sub-diagonal block appears twice in the symmetric matrix
+        prior_idx = [k for k in range(len(self.theta_keys)) if k not in self.tau_idx]
         fs, grads = [], []
         self.last_check = []
-        for sl, theta, tau in zip(sls, thetas, taus):
-            s = sl.scal[:5].cpu().numpy()
-            Ic = sl.inner_c.view(-1, 4).cpu().numpy()
-            Ip = sl.inner_p.view(-1, 4).cpu().numpy()
-            Qm = sl.quad_st.view(-1, 4).cpu().numpy()
+        for sl, theta in zip(sls, thetas):
+            s = sl.scal[:3].cpu().numpy()
+            vs = sl.vscal.view(-1, 3).cpu().numpy()
+            Ic = sl.inner_c.view(2 * n - 1, -1).cpu().numpy()
+            Ip = sl.inner_p.view(2 * n - 1, -1).cpu().numpy()
+            Qm = sl.quad_st.view(2 * n - 1, -1).cpu().numpy()
             Tsel = sl.Qc.T.cpu().numpy()
             f = 0.5 * s[0] - 0.5 * s[1] - (self.log_prior_theta(theta) + self.lik0(theta) + 0.5 * s[2])
             grad = np.zeros(theta.size)
-            for k in range(3):
+            for k in prior_idx:
                 dc = self._dcoef(theta, k) * mult
-                grad[k] = (0.5 * np.sum(dc * Ic) - 0.5 * np.sum(dc * Ip) + 0.5 * np.sum(dc * Qm)
+                grad[k] = 0.5 * np.sum(dc * (Ic - Ip + Qm)) - self._dfun(self.log_prior_theta, theta, k)
+            rest_c = 0.0
+            for j, k in enumerate(self.tau_idx):
+                tau = math.exp(theta[k])
+                tr_ata = vs[j, 0] + float(np.sum(Tsel * self.XtX_var[j]))
+                rest_c += tau * tr_ata
+                grad[k] = (0.5 * tau * tr_ata + 0.5 * tau * vs[j, 1] - tau * vs[j, 2]
+                           - (0.5 * self.nobs_var[j] - 0.5 * tau * self.yty_var[j])
                            - self._dfun(self.log_prior_theta, theta, k))
-            tr_ata = s[4] + float(np.sum(Tsel * self.XtX_host))
-            grad[-1] = (0.5 * tau * tr_ata - s[1] + 0.5 * tau * s[3]
-                        - (0.5 * self.nobs - 0.5 * tau * self.yty)
-                        - self._dfun(self.log_prior_theta, theta, theta.size - 1))
-            rc, rp = self._identity_residuals(theta, Ic, Ip, tau * tr_ata, self.fe_prec * float(np.trace(Tsel)))
+            rc, rp = self._identity_residuals(theta, Ic, Ip, rest_c, self.fe_prec * float(np.trace(Tsel)))
             self.last_check.append({"precision": precision, "residual_c": rc, "residual_p": rp, "fallback": False})
             fs.append(float(f))
             grads.append(grad)
@@ -625,7 +677,7 @@ class SpatioTemporalModel:
         if x_star is not None:
             sl.x.copy_(torch.as_tensor(np.asarray(x_star, dtype=np.float64)).to(self.device))
         if self.gaussian:
-            self.assemble_conditional(theta, None, math.exp(theta[-1]), sl)
+            self._gauss_conditional(theta, sl)
         else:
             self.spmv(self.A_rowptr, self.A_col, self.A_val, self.nobs, sl.x, sl.eta)
             self._check(self.lib.bta_poisson_terms(self._stream(), self.nobs, _lib.ptr(sl.eta), _lib.ptr(self.y),

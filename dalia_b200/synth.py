@@ -213,6 +213,104 @@ def make_problem(
     )
 
 
+@dataclasses.dataclass
+class CoregionalProblem:
+    """nv spatio-temporal variates on one mesh (the reference's
+    ``CoregionalModel``, ``src/dalia/models/coregional_model.py``), each with
+    its own observations, nb fixed effects and Gaussian likelihood.
+
+    theta follows the reference's order: per variate (r_s, r_t, prec_o),
+    then sigma_0..sigma_{nv-1}, then lambda_i_j for i < j."""
+
+    ns: int
+    nt: int
+    nv: int
+    nb: int  # fixed effects per variate
+    c0: sps.csc_matrix
+    g1: sps.csc_matrix
+    g2: sps.csc_matrix
+    g3: sps.csc_matrix
+    m0: sps.csc_matrix
+    m1: sps.csc_matrix
+    m2: sps.csc_matrix
+    a_st: list  # per variate (no_v*nt) x (ns*nt)
+    a_fe: list  # per variate (no_v*nt) x nb
+    y: list
+    theta: np.ndarray
+    sigma_st: np.ndarray  # fixed per-variate sigma_st of the submodels (not a hyperparameter)
+
+    @property
+    def theta_keys(self):
+        keys = []
+        for v in range(self.nv):
+            keys += [f"r_s_{v}", f"r_t_{v}", f"prec_o_{v}"]
+        keys += [f"sigma_{v}" for v in range(self.nv)]
+        keys += [f"lambda_{i}_{j}" for i in range(self.nv) for j in range(i + 1, self.nv)]
+        return keys
+
+
+def make_coregional_problem(ns, nt, nv, nb, no, theta, seed=0):
+    """Seeded synthetic coregional problem: one mesh and temporal FEM shared
+    by the variates, no observations per time step and variate, responses
+    y_v = A_v x_v + X_v beta_v + noise with x = mixtures of smooth fields."""
+    if nv not in (2, 3):
+        raise ValueError("nv must be 2 or 3")
+    rng = np.random.default_rng(seed)
+    pts, tri = _mesh(ns, rng)
+    c0, g1, g2, g3 = _fem(pts, tri.simplices)
+    m0, m1, m2 = _time_fem(nt)
+    theta = np.asarray(theta, dtype=np.float64)
+    a_st, a_fe, ys = [], [], []
+    # smooth fields u_k, mixed lower-triangularly into the variates
+    n_modes = 6
+    fields = []
+    for _ in range(nv):
+        kx = rng.uniform(0.5, 3.0, size=n_modes) * np.pi
+        ky = rng.uniform(0.5, 3.0, size=n_modes) * np.pi
+        ph = rng.uniform(0, 2 * np.pi, size=n_modes)
+        basis = np.cos(kx[None, :] * pts[:, :1] + ky[None, :] * pts[:, 1:2] + ph[None, :])
+        coef = np.zeros((nt, n_modes))
+        coef[0] = rng.standard_normal(n_modes)
+        for t in range(1, nt):
+            coef[t] = 0.9 * coef[t - 1] + math.sqrt(1 - 0.81) * rng.standard_normal(n_modes)
+        fields.append((coef @ basis.T).ravel() * 0.5)
+    for v in range(nv):
+        x_v = sum((0.5 ** (v - k)) * fields[k] for k in range(v + 1))
+        nobs = no * nt
+        obs_xy = rng.uniform(0.05, 0.95, size=(nobs, 2))
+        nodes, w = _barycentric(tri, obs_xy)
+        t_of = np.repeat(np.arange(nt), no)
+        rows = np.repeat(np.arange(nobs), 3)
+        cols = (t_of[:, None] * ns + nodes).ravel()
+        A = sps.coo_matrix((w.ravel(), (rows, cols)), shape=(nobs, ns * nt)).tocsc()
+        A.sum_duplicates()
+        X = rng.standard_normal((nobs, nb))
+        beta = rng.standard_normal(nb) * 0.3
+        tau = math.exp(theta[3 * v + 2])
+        ys.append(A @ x_v + X @ beta + rng.standard_normal(nobs) / math.sqrt(tau))
+        a_st.append(A)
+        a_fe.append(X)
+    return CoregionalProblem(ns=ns, nt=nt, nv=nv, nb=nb, c0=c0, g1=g1, g2=g2, g3=g3, m0=m0, m1=m1, m2=m2,
+                             a_st=a_st, a_fe=a_fe, y=ys, theta=theta, sigma_st=np.zeros(nv))
+
+
+def save_coregional_layout(prob: CoregionalProblem, root) -> None:
+    """One reference model directory per variate (``model_<v+1>/inputs_*``,
+    the layout of the reference's coregional examples) plus y per variate."""
+    import os
+
+    for v in range(prob.nv):
+        st = os.path.join(root, f"model_{v + 1}", "inputs_spatio_temporal")
+        rg = os.path.join(root, f"model_{v + 1}", "inputs_regression")
+        os.makedirs(st, exist_ok=True)
+        os.makedirs(rg, exist_ok=True)
+        for nm in ("c0", "g1", "g2", "g3", "m0", "m1", "m2"):
+            sps.save_npz(os.path.join(st, f"{nm}.npz"), getattr(prob, nm).tocsc())
+        sps.save_npz(os.path.join(st, "a.npz"), prob.a_st[v].tocsc())
+        sps.save_npz(os.path.join(rg, "a.npz"), sps.csc_matrix(prob.a_fe[v]))
+        np.save(os.path.join(root, f"model_{v + 1}", "y.npy"), prob.y[v])
+
+
 # Workloads with the reference examples' shapes (seed 0 each).
 CONFIGS = {
     "gst_300x10": dict(ns=300, nt=10, nb=4, no=200, theta=(-1.0, 1.0, 0.0, 2.0), likelihood="gaussian"),
@@ -225,7 +323,19 @@ CONFIGS = {
 }
 
 
-def make_config(name: str, seed: int = 0) -> SpatioTemporalProblem:
+# Coregional workloads: theta = per variate (r_s, r_t, prec_o), sigmas, lambdas.
+COREG_CONFIGS = {
+    "gst_coreg3_600x40": dict(ns=600, nt=40, nv=3, nb=1, no=200,
+                              theta=(-1.0, 1.0, 2.0, -0.8, 0.9, 1.8, -1.2, 1.1, 2.2,
+                                     0.0, 0.2, -0.1, 0.5, -0.3, 0.4)),
+    "gst_coreg2_600x40": dict(ns=600, nt=40, nv=2, nb=1, no=200,
+                              theta=(-1.0, 1.0, 2.0, -0.8, 0.9, 1.8, 0.0, 0.2, 0.5)),
+}
+
+
+def make_config(name: str, seed: int = 0):
+    if name in COREG_CONFIGS:
+        return make_coregional_problem(seed=seed, **COREG_CONFIGS[name])
     return make_problem(seed=seed, **CONFIGS[name])
 
 

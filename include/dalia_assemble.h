@@ -53,6 +53,19 @@ int bta_block_quad(void* stream, int64_t n, int64_t b, const int* rowptr, const 
 int bta_kron_symv(void* stream, int64_t n, int64_t b, const double* coef, const int* rowptr, const int* colidx,
                   const double* vals4, const double* x, double alpha, double beta, double* y);
 
+/* Multivariate forms (nv variates interleaved per time step, block size
+ * b = nv ns; the reference's CoregionalModel permutation,
+ * src/dalia/models/coregional_model.py:770-797): coef[blk][v][w][K] gives
+ * sub-block (v, w) = sum_K coef K of block blk; block_inner_mv and
+ * block_quad_mv return out[blk][v][w][K] (sub-block inner products with K, and
+ * x_{r,v}^T K x_{c,w}).  nv = 1 is the univariate form above. */
+int bta_assemble_prior_mv(void* stream, int64_t n, int64_t ns, int64_t nv, const double* coef, const int* rowptr,
+                          const int* colidx, const double* vals4, double* D, double* L);
+int bta_block_inner_mv(void* stream, int64_t n, int64_t ns, int64_t nv, const int* rowptr, const int* colidx,
+                       const double* vals4, const double* D, const double* L, double* out);
+int bta_block_quad_mv(void* stream, int64_t n, int64_t ns, int64_t nv, const int* rowptr, const int* colidx,
+                      const double* vals4, const double* x, double* out);
+
 /* Poisson likelihood at eta (src/dalia/likelihoods/poisson.py:35-63):
  * d = e exp(eta) (minus the Hessian diagonal), g = y - d (gradient),
  * *lik = eta . y - sum(e exp(eta)). */

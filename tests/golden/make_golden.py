@@ -46,6 +46,14 @@ CASES = {
 }
 
 
+COREG_CASES = {
+    # name: (ns, nt, nv, nb per variate, no, theta, seed)
+    "gst_coreg3_small": (40, 4, 3, 1, 30, (-1.0, 1.0, 2.0, -0.8, 0.9, 1.8, -1.2, 1.1, 2.2,
+                                           0.0, 0.2, -0.1, 0.5, -0.3, 0.4), 5),
+    "gst_coreg2_ragged": (70, 3, 2, 2, 40, (-0.9, 0.8, 1.5, -1.1, 1.2, 2.1, 0.1, -0.2, 0.6), 6),
+}
+
+
 def checksums(prob):
     out = {}
     for nm in ("c0", "g1", "g2", "g3", "m0", "m1", "m2", "a_st"):
@@ -175,6 +183,103 @@ def main(ref_root: str, only=None) -> None:
               f"diff={f_d - f_s:.6f} grad_serinv={np.asarray(g_s)}", flush=True)
 
 
+def coreg_checksums(prob):
+    out = {}
+    for nm in ("c0", "g1", "g2", "g3", "m0", "m1", "m2"):
+        d = getattr(prob, nm).tocsc().data
+        out[nm] = np.array([d.sum(), (d * d).sum(), d.size], dtype=np.float64)
+    for v in range(prob.nv):
+        d = prob.a_st[v].tocsc().data
+        out[f"a_st{v}"] = np.array([d.sum(), (d * d).sum(), d.size])
+        out[f"a_fe{v}"] = np.array([prob.a_fe[v].sum(), (prob.a_fe[v] ** 2).sum(), prob.a_fe[v].size])
+        out[f"y{v}"] = np.array([prob.y[v].sum(), (prob.y[v] ** 2).sum(), prob.y[v].size])
+    return out
+
+
+def main_coregional(ref_root: str, only=None) -> None:
+    """Coregional fixtures: the reference's ``CoregionalModel`` built from one
+    ``Model`` per variate (Gaussian priors as in its coregional examples),
+    driven through ``DALIA._objective_function`` with the dense and the
+    Serinv solvers."""
+    os.environ.setdefault("ARRAY_MODULE", "numpy")
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, os.path.join(ref_root, "src"))
+    from oracle import bta_ref
+
+    fake = types.ModuleType("serinv")
+    algs = types.ModuleType("serinv.algs")
+    for nm in ("pobtaf", "pobtas", "pobtasi", "pobtf", "pobts", "pobtsi"):
+        setattr(algs, nm, getattr(bta_ref, nm))
+    fake.algs = algs
+    sys.modules["serinv"] = fake
+    sys.modules["serinv.algs"] = algs
+
+    from dalia.configs import dalia_config, likelihood_config, models_config, submodels_config
+    from dalia.core.dalia import DALIA
+    from dalia.core.model import Model
+    from dalia.models import CoregionalModel
+    from dalia.submodels import RegressionSubModel, SpatioTemporalSubModel
+
+    from dalia_b200 import synth
+
+    g = lambda mean: {"type": "gaussian", "mean": float(mean), "precision": 0.5}
+    for name, (ns, nt, nv, nb, no, theta, seed) in COREG_CASES.items():
+        if only and name not in only:
+            continue
+        prob = synth.make_coregional_problem(ns, nt, nv, nb, no, theta, seed=seed)
+        th = np.asarray(theta, dtype=np.float64)
+        tmp = tempfile.mkdtemp(prefix=f"golden_{name}_")
+        synth.save_coregional_layout(prob, tmp)
+
+        def build(solver_type):
+            models = []
+            for v in range(nv):
+                mdir = f"{tmp}/model_{v + 1}"
+                st = SpatioTemporalSubModel(config=submodels_config.parse_config({
+                    "type": "spatio_temporal", "input_dir": f"{mdir}/inputs_spatio_temporal",
+                    "spatial_domain_dimension": 2, "r_s": th[3 * v], "r_t": th[3 * v + 1], "sigma_st": 0.0,
+                    "manifold": "plane", "ph_s": g(th[3 * v]), "ph_t": g(th[3 * v + 1]), "ph_st": g(0.0)}))
+                rg = RegressionSubModel(config=submodels_config.parse_config({
+                    "type": "regression", "input_dir": f"{mdir}/inputs_regression", "n_fixed_effects": nb,
+                    "fixed_effects_prior_precision": 0.001}))
+                lk = likelihood_config.parse_config({
+                    "type": "gaussian", "prec_o": th[3 * v + 2], "prior_hyperparameters": g(th[3 * v + 2])})
+                models.append(Model(submodels=[st, rg], likelihood_config=lk))
+            cfg = {"type": "coregional", "n_models": nv,
+                   "sigmas": [float(x) for x in th[3 * nv:4 * nv]],
+                   "lambdas": [float(x) for x in th[4 * nv:]],
+                   "ph_sigmas": [g(x) for x in th[3 * nv:4 * nv]],
+                   "ph_lambdas": [g(0.0) for _ in th[4 * nv:]]}
+            model = CoregionalModel(models=models, coregional_model_config=models_config.parse_config(cfg))
+            dal = DALIA(model=model, config=dalia_config.parse_config({
+                "solver": {"type": solver_type}, "inner_iteration_max_iter": 50,
+                "eps_inner_iteration": 1e-3, "eps_gradient_f": 1e-3, "simulation_dir": tmp}))
+            dal.iter = 0
+            return model, dal
+
+        out = {"theta": th, "shape": np.array([ns, nt, nv, nb, no, seed])}
+        for k, v in coreg_checksums(prob).items():
+            out[f"chk_{k}"] = v
+        model, dal = build("dense")
+        model.theta[:] = th
+        Qp = model.construct_Q_prior().tocoo()
+        Qc = model.construct_Q_conditional(np.zeros_like(model.y)).tocoo()
+        out["qp_row"], out["qp_col"], out["qp_data"] = Qp.row, Qp.col, Qp.data
+        out["qc_row"], out["qc_col"], out["qc_data"] = Qc.row, Qc.col, Qc.data
+        f_d, g_d = dal._objective_function(th.copy())
+        out["f_dense"], out["grad_dense"], out["x_dense"] = np.array(f_d), np.asarray(g_d), model.x.copy()
+        model, dal = build("serinv")
+        f_s, g_s = dal._objective_function(th.copy())
+        out["f_serinv"], out["grad_serinv"], out["x_serinv"] = np.array(f_s), np.asarray(g_s), model.x.copy()
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+        print(f"{name}: f_dense={f_d:.10f} f_serinv={f_s:.10f} diff={f_d - f_s:.6f}", flush=True)
+
+
 if __name__ == "__main__":
     # usage: make_golden.py [REF_ROOT [CASE ...]]
-    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DALIA_REF", "/root/reference"), sys.argv[2:])
+    _root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DALIA_REF", "/root/reference")
+    _only = sys.argv[2:]
+    if not _only or any(c in CASES for c in _only):
+        main(_root, [c for c in _only if c in CASES])
+    if not _only or any(c in COREG_CASES for c in _only):
+        main_coregional(_root, [c for c in _only if c in COREG_CASES])

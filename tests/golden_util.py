@@ -24,6 +24,22 @@ def problem(g):
     return prob
 
 
+def coreg_problem(g):
+    from dalia_b200 import synth
+
+    ns, nt, nv, nb, no, seed = (int(v) for v in g["shape"])
+    prob = synth.make_coregional_problem(ns, nt, nv, nb, no, tuple(g["theta"]), seed=seed)
+    for nm in ("c0", "g1", "g2", "g3", "m0", "m1", "m2"):
+        d = getattr(prob, nm).tocsc().data
+        np.testing.assert_allclose([d.sum(), (d * d).sum(), d.size], g[f"chk_{nm}"], rtol=1e-12)
+    for v in range(nv):
+        d = prob.a_st[v].tocsc().data
+        np.testing.assert_allclose([d.sum(), (d * d).sum(), d.size], g[f"chk_a_st{v}"], rtol=1e-12)
+        np.testing.assert_allclose([prob.y[v].sum(), (prob.y[v] ** 2).sum(), prob.y[v].size], g[f"chk_y{v}"],
+                                   rtol=1e-12)
+    return prob
+
+
 def rel(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
