@@ -66,13 +66,16 @@ def cpu_sample(workload, nt_sample, reps=1):
     """Time one f(theta) of the CPU oracle on the workload truncated to
     nt_sample time steps; returns (seconds per full FD gradient, description)."""
     from dalia_b200 import synth
-    from oracle import model_ref
+    from oracle import coreg_ref, model_ref
 
-    cfg = dict(synth.CONFIGS[workload])
+    coreg = workload in synth.COREG_CONFIGS
+    cfg = dict(synth.COREG_CONFIGS[workload] if coreg else synth.CONFIGS[workload])
     nt_full = cfg["nt"]
     cfg["nt"] = min(nt_sample, nt_full)
-    prob = synth.make_problem(seed=0, **cfg)
-    om = model_ref.OracleModel(prob)
+    if coreg:
+        om = coreg_ref.CoregionalOracle(synth.make_coregional_problem(seed=0, **cfg))
+    else:
+        om = model_ref.OracleModel(synth.make_problem(seed=0, **cfg))
     th = np.asarray(cfg["theta"], dtype=np.float64)
     om.evaluate_f(th)  # warm-up (BLAS thread pool, caches)
     ts = []
@@ -191,6 +194,7 @@ def run_ours(args):
     import torch
 
     from dalia_b200 import _lib, synth
+    from dalia_b200.coregional import CoregionalModel
     from dalia_b200.model import SpatioTemporalModel
 
     rank, world, local = dist_info()
@@ -201,10 +205,11 @@ def run_ours(args):
     dev = torch.device("cuda", torch.cuda.current_device())
     lib = _lib.load()
 
-    cfg = synth.CONFIGS[args.workload]
+    coreg = args.workload in synth.COREG_CONFIGS
+    cfg = synth.COREG_CONFIGS[args.workload] if coreg else synth.CONFIGS[args.workload]
     prob = synth.make_config(args.workload, seed=0)
-    model = SpatioTemporalModel(prob, device=dev)
-    n, b, a = model.nt, model.ns, model.nb
+    model = (CoregionalModel if coreg else SpatioTemporalModel)(prob, device=dev)
+    n, b, a = model.nt, model.b, model.nb
     # replicas evaluate different theta points (a line-search batch)
     theta = np.asarray(cfg["theta"], dtype=np.float64) + 1e-3 * rank
 
@@ -297,6 +302,17 @@ def run_ours(args):
         f1.record()
         barrier()
         fd_rate = args.fd_steps / (f0.elapsed_time(f1) * 1e-3)
+    # the same stencil with its 2d+1 points factorised in batches (Gaussian)
+    fdb_rate = None
+    if args.fd_steps > 0 and model.gaussian:
+        barrier()
+        f0, f1 = torch.cuda.Event(True), torch.cuda.Event(True)
+        f0.record()
+        for _ in range(args.fd_steps):
+            model.objective_fd_batched(theta)
+        f1.record()
+        barrier()
+        fdb_rate = args.fd_steps / (f0.elapsed_time(f1) * 1e-3)
 
     # ---- roofline of the dominant kernel category
     names = {0: "panel (tile-DAG BTA panel Cholesky)", 1: "gemm (grouped FP64 DMMA GEMM)"}
@@ -350,12 +366,13 @@ def run_ours(args):
             "data": "synthetic",
             "config": {
                 "workload": args.workload,
-                "ns": b, "nt": n, "nb": a, "obs_per_step": cfg["no"], "theta": list(cfg["theta"]),
+                "ns": model.ns, "variates": model.nv, "block": b, "nt": n, "nb": a, "obs_per_step": cfg["no"],
+                "theta": list(cfg["theta"]),
                 "path": f"adjoint gradient, FP64; {K} theta points per step (line-search batch), theta moved "
                         f"between steps; Q_c and Q_prior of all points factorised and selected-inverted together",
                 "theta_points_per_step": K,
                 "parallelism": f"replicas x{world}",
-                "likelihood": cfg["likelihood"],
+                "likelihood": cfg.get("likelihood", "gaussian"),
                 "l2": f"inputs larger than L2 (BTA matrix {model.Qc.buf.numel() * 8 / 1e9:.1f} GB each)",
             },
             "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -364,6 +381,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "clocks": clocks,
             "fd_fp64_evals_per_s": fd_rate,
+            "fd_fp64_batched_stencil_evals_per_s": fdb_rate,
             "adjoint_single_point_evals_per_s": single_rate,
             "speedup_vs_fd_fp64": (value / fd_rate) if fd_rate else None,
             "bta_factor_tflops": tot_flops[0] / (ms_cat[0] * 1e-3) / 1e12,

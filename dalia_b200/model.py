@@ -538,6 +538,61 @@ class SpatioTemporalModel:
             fv[k] = self.evaluate_f(tm[:, k])
         return fv[0], (fv[1:1 + d] - fv[d + 1:nf]) / (2 * self.eps)
 
+    def evaluate_f_batched(self, thetas):
+        """f at K theta points with all 2K factorisations (Q_c and Q_prior of
+        every point) in one batched launch sequence (Gaussian likelihoods,
+        whose evaluations carry no state from point to point).  model.x ends
+        as the latent mean of the first point."""
+        if not self.gaussian:
+            raise NotImplementedError("batched f: Gaussian likelihoods (the Newton iteration is warm-started "
+                                      "from point to point)")
+        thetas = [np.asarray(t, dtype=np.float64) for t in thetas]
+        sls = [self.slot(j) for j in range(len(thetas))]
+        _lib.check(self.lib.bta_reset_status(self.h.bind_stream()), "reset")
+        for sl, th in zip(sls, thetas):
+            self._gauss_conditional(th, sl)
+            self.assemble_prior_bt(th, sl)
+        self.factor_batched([sl.Qc for sl in sls] + [sl.Qp for sl in sls])
+        for sl, th in zip(sls, thetas):
+            self.logdet_to(sl.Qc, sl.scal[0:1])
+            self.logdet_to(sl.Qp, sl.scal[2:3])
+            self._gauss_rhs(th, sl)
+            sl.x.copy_(sl.rhs)
+        self.sweep_batched([sl.Qc for sl in sls], [sl.x for sl in sls], 0)
+        for sl in sls:
+            self.dot_to(sl.x, sl.x, sl.scal[1:2])  # b^T Q_c^-1 b = mu^T Q_c mu
+        self.sweep(sls[0].Qc, sls[0].x, 1)
+        self.status()
+        fs = []
+        for sl, th in zip(sls, thetas):
+            v = sl.scal[:3].cpu().numpy()
+            f = 0.5 * v[0] - 0.5 * v[1] - (self.log_prior_theta(th) + self.lik0(th) + 0.5 * v[2])
+            if np.isnan(f):
+                raise ValueError("f(theta) is NaN. Check what is happening.")
+            fs.append(float(f))
+        return fs
+
+    def objective_fd_batched(self, theta, max_points=16):
+        """The reference's central-difference objective (``dalia.py:513-601``)
+        with the 2d+1 stencil points evaluated in batches of up to
+        max_points (Gaussian likelihoods); the same values as
+        ``objective_fd``."""
+        theta = np.asarray(theta, dtype=np.float64)
+        d = theta.size
+        nf = 2 * d + 1
+        tm = np.repeat(theta.reshape(-1, 1), nf, axis=1)
+        tm[:, 1:1 + d] += self.eps * np.eye(d)
+        tm[:, d + 1:nf] -= self.eps * np.eye(d)
+        fv = np.zeros(nf)
+        # the centre goes last and first in its batch, so that model.x is its latent mean
+        order = list(range(1, nf)) + [0]
+        for c0 in range(0, nf, max_points):
+            idx = order[c0:c0 + max_points]
+            if 0 in idx:
+                idx = [0] + [i for i in idx if i != 0]
+            fv[idx] = self.evaluate_f_batched([tm[:, i] for i in idx])
+        return fv[0], (fv[1:1 + d] - fv[d + 1:nf]) / (2 * self.eps)
+
     def _dcoef(self, theta, k):
         th = np.asarray(theta, dtype=np.complex128).copy()
         th[k] += 1j * _CSTEP

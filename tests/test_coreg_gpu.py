@@ -67,3 +67,15 @@ def test_marginal_variances():
     Ad = orc.A.toarray()
     mo = m.marginal_variances_observations(g["theta"]).cpu().numpy()
     assert rel(mo, np.einsum("ij,jk,ik->i", Ad, S, Ad)) < 1e-10
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_batched_fd_stencil_matches_sequential(name):
+    from dalia_b200.coregional import CoregionalModel
+
+    g = load(name)
+    m = CoregionalModel(coreg_problem(g))
+    f, grad = m.objective_fd_batched(g["theta"], max_points=8)
+    assert abs(f - float(g["f_serinv"])) < 1e-10 * max(1.0, abs(float(g["f_serinv"])))
+    assert rel(grad, g["grad_serinv"]) < 1e-7
+    assert rel(m.x.cpu().numpy(), g["x_serinv"]) < 1e-10

@@ -132,3 +132,14 @@ def test_marginal_variances(name):
         assert rel(mv, g["marg_var_serinv"]) < 1e-10
     mo = m.marginal_variances_observations(th, x).cpu().numpy()
     assert rel(mo, np.einsum("ij,jk,ik->i", Ad, S, Ad)) < 1e-10
+
+
+def test_batched_fd_stencil_matches_reference():
+    from dalia_b200.model import SpatioTemporalModel
+
+    g = load("gst_300x10")
+    m = SpatioTemporalModel(problem(g))
+    f, grad = m.objective_fd_batched(g["theta"])
+    assert abs(f - float(g["f_serinv"])) < 1e-10 * abs(float(g["f_serinv"]))
+    assert rel(grad, g["grad_serinv"]) < 1e-7
+    assert rel(m.x.cpu().numpy(), g["x_serinv"]) < 1e-10
