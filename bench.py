@@ -53,6 +53,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-oracle baseline sample")
     p.add_argument("--batch", type=int, default=3,
                    help="theta points per step (a line-search batch), factorised together")
+    p.add_argument("--precision", default="i8slice", choices=["fp64", "tf32x3", "i8slice"],
+                   help="arithmetic of the selected inversions behind the adjoint gradient")
     return p.parse_args()
 
 
@@ -208,7 +210,7 @@ def run_ours(args):
     coreg = args.workload in synth.COREG_CONFIGS
     cfg = synth.COREG_CONFIGS[args.workload] if coreg else synth.CONFIGS[args.workload]
     prob = synth.make_config(args.workload, seed=0)
-    model = (CoregionalModel if coreg else SpatioTemporalModel)(prob, device=dev)
+    model = (CoregionalModel if coreg else SpatioTemporalModel)(prob, device=dev, selinv_precision=args.precision)
     n, b, a = model.nt, model.b, model.nb
     # replicas evaluate different theta points (a line-search batch)
     theta = np.asarray(cfg["theta"], dtype=np.float64) + 1e-3 * rank
@@ -245,8 +247,12 @@ def run_ours(args):
     barrier()
     e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
     e0.record()
+    fallbacks = 0
+    resid_max = 0.0
     for s in range(args.steps):
         model.objective_adjoint_batched(step_th[s])
+        fallbacks += sum(1 for c in model.last_check if c["fallback"])
+        resid_max = max([resid_max] + [max(c["residual_c"], c["residual_p"]) for c in model.last_check])
     e1.record()
     barrier()
     launches = lib.bta_launch_count() - launches0
@@ -292,6 +298,15 @@ def run_ours(args):
     d2h = K * ((5 + 3 * (2 * n - 1) * 4 + a * a) * 8) + 16
 
     # ---- plain FP64 finite differences (the reference's algorithm)
+    # accuracy of the reduced-precision selected inversion against FP64 at one
+    # point (outside every timed region)
+    accuracy = {"fallbacks_in_timed_region": fallbacks, "max_identity_residual": resid_max}
+    if args.precision != "fp64":
+        fr, gr = model.objective_adjoint_batched([theta])
+        f64, g64 = model.objective_adjoint_batched([theta], precision="fp64")
+        accuracy["grad_rel_err_vs_fp64"] = float(np.linalg.norm(np.asarray(gr[0]) - np.asarray(g64[0]))
+                                                 / np.linalg.norm(np.asarray(g64[0])))
+        accuracy["f_rel_err_vs_fp64"] = abs(fr[0] - f64[0]) / abs(f64[0])
     fd_rate = None
     if args.fd_steps > 0:
         barrier()
@@ -362,13 +377,14 @@ def run_ours(args):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f64",
+            "dtype": "f64" if args.precision == "fp64" else f"f64 + {args.precision} block products",
             "data": "synthetic",
             "config": {
                 "workload": args.workload,
                 "ns": model.ns, "variates": model.nv, "block": b, "nt": n, "nb": a, "obs_per_step": cfg["no"],
                 "theta": list(cfg["theta"]),
-                "path": f"adjoint gradient, FP64; {K} theta points per step (line-search batch), theta moved "
+                "path": f"adjoint gradient, selected inversion in {args.precision} (factorisations, log-dets, solves "
+                        f"FP64); {K} theta points per step (line-search batch), theta moved "
                         f"between steps; Q_c and Q_prior of all points factorised and selected-inverted together",
                 "theta_points_per_step": K,
                 "parallelism": f"replicas x{world}",
@@ -380,6 +396,7 @@ def run_ours(args):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks,
+            "mixed_accuracy": accuracy,
             "fd_fp64_evals_per_s": fd_rate,
             "fd_fp64_batched_stencil_evals_per_s": fdb_rate,
             "adjoint_single_point_evals_per_s": single_rate,

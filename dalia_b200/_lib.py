@@ -32,6 +32,7 @@ _dbl = ctypes.c_double
 
 BTA_PREC_FP64 = 0
 BTA_PREC_TF32X3 = 1
+BTA_PREC_I8SLICE = 2
 
 SIGNATURES = {
     "bta_create": (_int, [ctypes.POINTER(_c_void_p)]),

@@ -20,6 +20,8 @@ struct bta_context {
   cudaStream_t stream = nullptr;
   char* ws = nullptr;
   size_t ws_bytes = 0;
+  char* ws2 = nullptr;  // digit images of the 8-bit-slice GEMM
+  size_t ws2_bytes = 0;
   int* ctl = nullptr;  // [0] abort flag, [1] scratch; ctl+2 (8-aligned): info (u64)
   double* scal = nullptr;
   std::map<std::vector<int>, std::pair<int4*, int>> tasks;
@@ -40,6 +42,36 @@ struct Carve {
     return p;
   }
 };
+
+int ensure_ws2(bta_context* h, size_t bytes) {
+  if (bytes <= h->ws2_bytes) return BTA_OK;
+  if (h->ws2) {
+    cudaStreamSynchronize(h->stream);
+    cudaFree(h->ws2);
+    h->ws2 = nullptr;
+    h->ws2_bytes = 0;
+  }
+  size_t want = align_up(bytes + (bytes >> 3));
+  if (cudaMalloc(&h->ws2, want) != cudaSuccess) {
+    cudaGetLastError();
+    return BTA_ERR_ALLOC;
+  }
+  h->ws2_bytes = want;
+  return BTA_OK;
+}
+
+// Grouped GEMM in the requested arithmetic on the handle's stream.
+int run_gemm(bta_context* h, const std::vector<GemmProb>& pr, int precision) {
+  if (precision == BTA_PREC_TF32X3) return gemm_launch_tc(pr, h->stream, h->ctl) ? BTA_ERR_CUDA : BTA_OK;
+  if (precision == BTA_PREC_I8SLICE) {
+    size_t need = 0;
+    if (gemm_launch_i8(pr, h->stream, h->ctl, nullptr, 0, &need)) return BTA_ERR_INVALID;
+    int rc = ensure_ws2(h, need);
+    if (rc) return rc;
+    return gemm_launch_i8(pr, h->stream, h->ctl, h->ws2, h->ws2_bytes, nullptr) ? BTA_ERR_CUDA : BTA_OK;
+  }
+  return gemm_launch(pr, h->stream) ? BTA_ERR_CUDA : BTA_OK;
+}
 
 int ensure_ws(bta_context* h, size_t bytes) {
   if (bytes <= h->ws_bytes) return BTA_OK;
@@ -250,6 +282,7 @@ int bta_destroy(bta_handle_t h) {
   cudaStreamSynchronize(h->stream);
   for (auto& kv : h->tasks) cudaFree(kv.second.first);
   if (h->ws) cudaFree(h->ws);
+  if (h->ws2) cudaFree(h->ws2);
   cudaFree(h->ctl);
   cudaFree(h->scal);
   delete h;
@@ -402,11 +435,10 @@ int bta_pobtasi_batched_ex(bta_handle_t h, int count, const int64_t* n, const in
                            double* const* D, double* const* L, double* const* Ab, double* const* T,
                            int precision) {
   if (!h || count < 1 || !n || !b || !a || !D) return BTA_ERR_INVALID;
-  if (precision != BTA_PREC_FP64 && precision != BTA_PREC_TF32X3) return BTA_ERR_INVALID;
-  // the b x b block products go to the tensor-core kernel in TF32x3 mode
-  auto launch = [&](const std::vector<GemmProb>& pr) {
-    return precision == BTA_PREC_TF32X3 ? gemm_launch_tc(pr, h->stream, h->ctl) : gemm_launch(pr, h->stream);
-  };
+  if (precision != BTA_PREC_FP64 && precision != BTA_PREC_TF32X3 && precision != BTA_PREC_I8SLICE)
+    return BTA_ERR_INVALID;
+  // the block products go to the grouped GEMM of the requested arithmetic
+  auto launch = [&](const std::vector<GemmProb>& pr) { return run_gemm(h, pr, precision); };
   size_t need = 8 * kAlign;
   int64_t maxn = 0;
   for (int k = 0; k < count; ++k) {
@@ -488,9 +520,9 @@ int bta_pobtasi_batched_ex(bta_handle_t h, int count, const int64_t* n, const in
       if (a[k] > 0) gemm_add(r, w[k].Ga, B_, Abi, B_, A_, -1.0, GF_A_T | GF_B_KN);
       pc.push_back(r);
     }
-    if (!pa.empty() && launch(pa)) return BTA_ERR_CUDA;
-    if (!pb.empty() && launch(pb)) return BTA_ERR_CUDA;
-    if (!pc.empty() && launch(pc)) return BTA_ERR_CUDA;
+    if (!pa.empty() && (rc = launch(pa))) return rc;
+    if (!pb.empty() && (rc = launch(pb))) return rc;
+    if (!pc.empty() && (rc = launch(pc))) return rc;
     for (int k = 0; k < count; ++k) {
       const int64_t i = n[k] - 1 - st;
       if (i < 0) continue;
@@ -511,15 +543,15 @@ int bta_gemm(bta_handle_t h, int precision, int64_t M, int64_t N, int64_t K, dou
              int64_t lda, int a_trans, const double* B, int64_t ldb, int b_kn, double beta, double* C, int64_t ldc,
              int lower_only, int mirror) {
   if (!h || M < 0 || N < 0 || K < 0 || M > INT32_MAX || N > INT32_MAX || K > INT32_MAX) return BTA_ERR_INVALID;
-  if (precision != BTA_PREC_FP64 && precision != BTA_PREC_TF32X3) return BTA_ERR_INVALID;
+  if (precision != BTA_PREC_FP64 && precision != BTA_PREC_TF32X3 && precision != BTA_PREC_I8SLICE)
+    return BTA_ERR_INVALID;
   if (M == 0 || N == 0) return BTA_OK;
   if (!C || ldc < N || (lower_only && M != N) || (mirror && !lower_only)) return BTA_ERR_INVALID;
   if (K > 0 && (!A || !B || lda < (a_trans ? M : K) || ldb < (b_kn ? N : K))) return BTA_ERR_INVALID;
   GemmProb p = gemm_prob(C, (int)ldc, (int)M, (int)N, beta, (lower_only ? GC_LOWER : 0) | (mirror ? GC_MIRROR : 0));
   if (K > 0) gemm_add(p, A, (int)lda, B, (int)ldb, (int)K, alpha, (a_trans ? GF_A_T : 0) | (b_kn ? GF_B_KN : 0));
   std::vector<GemmProb> v{p};
-  const int e = precision == BTA_PREC_TF32X3 ? gemm_launch_tc(v, h->stream, h->ctl) : gemm_launch(v, h->stream);
-  return e == 0 ? BTA_OK : BTA_ERR_CUDA;
+  return run_gemm(h, v, precision);
 }
 
 int bta_logdet(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D, const double* T, int include_tip,

@@ -63,6 +63,12 @@ int gemm_launch(const std::vector<GemmProb>& probs, cudaStream_t stream);
 // bounded wait inside the kernel gives up.
 int gemm_launch_tc(const std::vector<GemmProb>& probs, cudaStream_t stream, int* abort_flag);
 
+// The same problems with 8-bit digit products accumulated exactly in INT32
+// (gemm_i8.cu).  With ws == nullptr only *ws_needed (bytes of workspace for
+// the exponents and digit images) is set; otherwise ws must hold that many.
+int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int* abort_flag, void* ws,
+                   size_t ws_bytes, size_t* ws_needed);
+
 inline GemmProb gemm_prob(double* C, int ldc, int M, int N, double beta, int cflags = 0) {
   GemmProb p{};
   p.C = C;

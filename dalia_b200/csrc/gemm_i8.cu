@@ -1,0 +1,579 @@
+// Grouped GEMM with near-FP64 accuracy from 8-bit tensor-core products
+// (tcgen05.mma kind::i8, exact INT32 accumulation in tensor memory): the
+// Ozaki splitting scheme.
+//
+// Every row m of op(A) (over all segments of a problem) gets one power-of-two
+// scale 2^e_m with max_k |alpha A[m][k]| < 2^e_m, every column n of op(B) one
+// scale 2^f_n; the scaled entries lie in (-1, 1) and are cut into OZ_S signed
+// 7-bit digits (truncation: |x 2^-e - sum_p a_p 2^-7p| < 2^-7 OZ_S).  Then
+//   C[m][n] = beta C + 2^(e_m + f_n) sum_{d} 2^-7d sum_{p+q=d} (a_p . b_q)
+// where every digit product sum is exact in INT32 (|a_p b_q| <= 127^2, at
+// most OZ_S pairs per d, K <= 19000).  Keeping d <= OZ_S + 1 drops terms
+// below 2^-7(OZ_S+1) 127^2 per element product: a relative error of ~1e-14
+// against sum_k |a||b| for OZ_S = 7.  Seven digits are needed because the
+// selected inversion of an ill-conditioned precision (cond ~1e9 per block)
+// amplifies the truncation: five digits left gradient errors of 2e-3 at
+// b = 1500.
+//
+// Pipeline: slice_exp_kernel (row / column maxima -> exponents, atomicMax),
+// slice_kernel (digits, written as the 32-byte-swizzled K-major shared-memory
+// images the MMA reads), gemm_i8_kernel: one producer thread bulk-copies the
+// digit images of a 32-wide k-slab (A: 128 rows x OZ_S digits, B: 64 rows x
+// OZ_S digits, no multicast) into a 4-stage ring; one thread issues the 28
+// (p, q) MMAs of the slab, each into the TMEM accumulator of d = p + q; four
+// epilogue warps read the OZ_S accumulators (tcgen05.ld), rescale and write C
+// in FP64.  Every wait is bounded and raises the abort flag on timeout.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "gemm.cuh"
+#include "prof.cuh"
+
+namespace bta {
+namespace {
+
+constexpr int OZ_S = 7;                        // digits per operand
+constexpr int QBM = 128, QBN = 64, QBK = 32;   // output tile, k-slab (32 int8 = one 32-byte row)
+constexpr int IMG = 64 * QBK;                  // one 64-row digit image (2 KB)
+constexpr int QSTAGES = 4;
+constexpr int A_SLICE = 2 * IMG;               // 128 rows
+constexpr int B_SLICE = IMG;                   // 64 rows
+constexpr int QSTAGE_BYTES = OZ_S * (A_SLICE + B_SLICE);
+constexpr int QTHREADS = 6 * 32;               // 4 epilogue warps, producer warp, MMA warp
+constexpr size_t QSMEM_BYTES = size_t(QSTAGES) * QSTAGE_BYTES + 256 + 1024;
+constexpr int TMEM_COLS = 512;                 // OZ_S accumulators of QBN columns
+constexpr long long QWAIT_CYCLES = 4000000000LL;
+constexpr int EXP_NONE = -1100;                // exponent of an all-zero row
+static_assert(OZ_S * QBN <= TMEM_COLS, "accumulators exceed tensor memory");
+
+// Instruction descriptor: D S32 (bits 4-5 = 2), A and B signed 8-bit (bits
+// 7-9, 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
+constexpr uint32_t IDESC_I8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(QBN >> 3) << 17) |
+                              ((uint32_t)(QBM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// K-major operand in the 32-byte swizzle layout: rows of 32 bytes, 8-row
+// groups 256 bytes apart, descriptor version 1, layout type 6 (SWIZZLE_32B).
+__device__ __forceinline__ uint64_t sw32_desc(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(256 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)6 << 61);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ bool mbar_wait(uint32_t bar, uint32_t parity, int* abort_flag) {
+  if (mbar_try(bar, parity)) return true;
+  const long long t0 = clock64();
+  for (int it = 1;; ++it) {
+    if (mbar_try(bar, parity)) return true;
+    if ((it & 63) == 0) {
+      if (*reinterpret_cast<volatile int*>(abort_flag)) return false;
+      if (clock64() - t0 > QWAIT_CYCLES) {
+        atomicExch(abort_flag, 1);
+        return false;
+      }
+    }
+  }
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(IDESC_I8), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = (int)r[i];
+}
+
+// ---------------------------------------------------------------- slicing
+// One operand of one segment: rows x K, element (r, k) at P[r*ld + k]
+// (kcontig) or P[k*ld + r], scaled by alpha; digits go to
+// out[(p*KT + kt)*RB + rb] (one 2 KB image per 64 rows x 32 k), exponents to
+// exps[rows] (shared by all segments of a problem).
+struct SliceJob {
+  const double* P;
+  double alpha;
+  int* exps;
+  int8_t* out;
+  int ld, rows, K, kcontig, RB, KT;
+  int unit_start;   // first work unit of this job (exponent pass)
+  int chunk_start;  // first 16-byte chunk of this job (digit pass)
+};
+
+constexpr int SLICE_MAXJ = 160;
+constexpr int EXP_KCHUNK = 256;
+
+struct SliceBatch {
+  int count;
+  int units;
+  int chunks;
+  SliceJob job[SLICE_MAXJ];
+};
+
+__device__ __forceinline__ int find_job(const SliceBatch& B, int idx, bool units) {
+  int j = 0;
+  while (j + 1 < B.count && idx >= (units ? B.job[j + 1].unit_start : B.job[j + 1].chunk_start)) ++j;
+  return j;
+}
+
+__device__ __forceinline__ int exponent_of(double m) {
+  if (!(m > 0.0)) return EXP_NONE;
+  int e;
+  frexp(m, &e);  // m = f 2^e, f in [0.5, 1): m < 2^e
+  return e;
+}
+
+// Work unit: (job, group of 32 rows, chunk of EXP_KCHUNK k); one warp, one
+// lane per row of the group; combined over units and segments by atomicMax.
+__global__ void __launch_bounds__(256) slice_exp_kernel(const __grid_constant__ SliceBatch B) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < B.units; u += warps) {
+    const SliceJob& J = B.job[find_job(B, u, true)];
+    const int local = u - J.unit_start;
+    const int nkc = max(1, (J.K + EXP_KCHUNK - 1) / EXP_KCHUNK);
+    const int g = local / nkc, kc = local - g * nkc;
+    const int r0 = g * 32, k0 = kc * EXP_KCHUNK, k1 = min(J.K, k0 + EXP_KCHUNK);
+    double mymax = 0.0;
+    if (J.kcontig) {
+      for (int rr = 0; rr < 32 && r0 + rr < J.rows; ++rr) {
+        const double* row = J.P + (size_t)(r0 + rr) * J.ld;
+        double m = 0.0;
+        for (int k = k0 + lane; k < k1; k += 32) m = fmax(m, fabs(row[k]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == rr) mymax = m;
+      }
+    } else if (r0 + lane < J.rows) {
+      for (int k = k0; k < k1; ++k) mymax = fmax(mymax, fabs(J.P[(size_t)k * J.ld + r0 + lane]));
+    }
+    if (r0 + lane < J.rows) atomicMax(&J.exps[r0 + lane], exponent_of(fabs(J.alpha) * mymax));
+  }
+}
+
+// One thread per 16-byte chunk (row r, k = 16c .. 16c + 15) for all OZ_S
+// digits; K-contiguous operands map consecutive threads along k, the others
+// along rows, so the FP64 reads coalesce.
+__global__ void __launch_bounds__(256) slice_kernel(const __grid_constant__ SliceBatch B) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < B.chunks; q += gridDim.x * blockDim.x) {
+    const SliceJob& J = B.job[find_job(B, q, false)];
+    const int local = q - J.chunk_start;
+    const int nrow = J.RB * 64, nkc = 2 * J.KT;
+    int r, kc;
+    if (J.kcontig) {
+      r = local / nkc;
+      kc = local - r * nkc;
+    } else {
+      kc = local / nrow;
+      r = local - kc * nrow;
+    }
+    const int k0 = kc * 16;
+    const int e = r < J.rows ? max(J.exps[r], EXP_NONE) : EXP_NONE;
+    uint32_t w[OZ_S][4];
+#pragma unroll
+    for (int p = 0; p < OZ_S; ++p)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) w[p][i] = 0u;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int k = k0 + j;
+      double x = 0.0;
+      if (r < J.rows && k < J.K) x = J.P[J.kcontig ? (size_t)r * J.ld + k : (size_t)k * J.ld + r];
+      x *= J.alpha;
+      const unsigned long long U = __double2ull_rz(ldexp(fabs(x), 7 * OZ_S - e));
+      const bool neg = x < 0.0;
+#pragma unroll
+      for (int p = 0; p < OZ_S; ++p) {
+        int dgt = (int)((U >> (7 * (OZ_S - 1 - p))) & 127ull);
+        if (neg) dgt = -dgt;
+        w[p][j >> 2] |= ((uint32_t)(uint8_t)(int8_t)dgt) << (8 * (j & 3));
+      }
+    }
+    const int kt = kc >> 1, c = kc & 1, rb = r >> 6, rr = r & 63;
+    const size_t off = (size_t)rr * 32 + ((size_t)(c ^ ((rr >> 2) & 1)) << 4);
+#pragma unroll
+    for (int p = 0; p < OZ_S; ++p) {
+      int8_t* dst = J.out + (((size_t)p * J.KT + kt) * J.RB + rb) * IMG + off;
+      *reinterpret_cast<uint4*>(dst) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- GEMM
+struct QSeg {
+  const int8_t* A;  // digit images of op(A): OZ_S x KT x RBa images
+  const int8_t* B;  // digit images of op(B): OZ_S x KT x RBb images
+  int KT, RBa, RBb, kflags, K;
+};
+
+struct QProb {
+  double* C;
+  const int* eA;  // M row exponents
+  const int* fB;  // N column exponents
+  double beta;
+  int ldc, M, N, nseg, cflags, tmn, tnn;
+  QSeg seg[3];
+};
+
+constexpr int QMAXP = 48;
+
+struct QBatch {
+  int count;
+  int tile_start[QMAXP + 1];
+  QProb p[QMAXP];
+};
+
+// lower-only tiles: (tm, tn) with tn * QBN <= tm * QBM + QBM - 1
+__device__ __forceinline__ int lower_tiles_row(int tm, int tnn) { return min(2 * tm + 2, tnn); }
+
+__device__ __forceinline__ int qseg_range(const QSeg& s, int m0, int n0, int& kt0) {
+  int kmin = 0, kmax = s.K;
+  if (s.kflags & GF_K_GE_M) kmin = max(kmin, m0);
+  if (s.kflags & GF_K_GE_N) kmin = max(kmin, n0);
+  if (s.kflags & GF_K_LE_M) kmax = min(kmax, m0 + QBM);
+  if (s.kflags & GF_K_LE_N) kmax = min(kmax, n0 + QBN);
+  kt0 = kmin / QBK;
+  const int kt1 = (kmax + QBK - 1) / QBK;
+  return kt1 > kt0 ? kt1 - kt0 : 0;
+}
+
+__global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_constant__ QBatch batch, int* abort_flag) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  uint8_t* bars = smem + QSTAGES * QSTAGE_BYTES;
+  const uint32_t full0 = smem_u32(bars), empty0 = full0 + 8 * QSTAGES, done_bar = empty0 + 8 * QSTAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 8 * (2 * QSTAGES + 1));
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int bid = blockIdx.x;
+  int pi = 0;
+  while (pi + 1 < batch.count && bid >= batch.tile_start[pi + 1]) ++pi;
+  const QProb& P = batch.p[pi];
+  int local = bid - batch.tile_start[pi];
+  int tm = 0, tn = 0;
+  if (P.cflags & GC_LOWER) {
+    while (local >= lower_tiles_row(tm, P.tnn)) local -= lower_tiles_row(tm++, P.tnn);
+    tn = local;
+  } else {
+    tm = local / P.tnn;
+    tn = local - tm * P.tnn;
+  }
+  const int m0 = tm * QBM, n0 = tn * QBN;
+
+  if (warp == 5) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"((uint32_t)TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < QSTAGES; ++s) {
+      mbar_init(full0 + 8 * s, 1);
+      mbar_init(empty0 + 8 * s, 1);
+    }
+    mbar_init(done_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  int nsteps = 0;
+  for (int si = 0; si < P.nseg; ++si) {
+    int kt0;
+    nsteps += qseg_range(P.seg[si], m0, n0, kt0);
+  }
+  const uint32_t stage0 = smem_u32(smem);
+
+  if (warp == 4) {
+    // ------------------------------------------------------ producer
+    if (lane == 0) {
+      int step = 0;
+      bool ok = true;
+      for (int si = 0; si < P.nseg && ok; ++si) {
+        const QSeg& s = P.seg[si];
+        int kt0;
+        const int nk = qseg_range(s, m0, n0, kt0);
+        for (int i = 0; i < nk; ++i, ++step) {
+          const int st = step % QSTAGES;
+          if (step >= QSTAGES && !mbar_wait(empty0 + 8 * st, ((step / QSTAGES) - 1) & 1, abort_flag)) {
+            ok = false;
+            break;
+          }
+          const int kt = kt0 + i;
+          const uint32_t bar = full0 + 8 * st;
+          mbar_expect_tx(bar, QSTAGE_BYTES);
+          const uint32_t dst = stage0 + st * QSTAGE_BYTES;
+#pragma unroll
+          for (int p = 0; p < OZ_S; ++p) {
+            bulk_g2s(dst + p * A_SLICE, s.A + (((size_t)p * s.KT + kt) * s.RBa + 2 * tm) * IMG, A_SLICE, bar);
+            bulk_g2s(dst + OZ_S * A_SLICE + p * B_SLICE, s.B + (((size_t)p * s.KT + kt) * s.RBb + tn) * IMG,
+                     B_SLICE, bar);
+          }
+        }
+      }
+    }
+  } else if (warp == 5) {
+    // ------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      for (int step = 0; step < nsteps; ++step) {
+        const int st = step % QSTAGES;
+        if (!mbar_wait(full0 + 8 * st, (step / QSTAGES) & 1, abort_flag)) break;
+        tc_fence_after();
+        const uint32_t a0 = stage0 + st * QSTAGE_BYTES, b0 = a0 + OZ_S * A_SLICE;
+#pragma unroll
+        for (int p = 0; p < OZ_S; ++p)
+#pragma unroll
+          for (int q = 0; q + p < OZ_S; ++q) {
+            // digits p, q (0-based): accumulator d = p + q; its first product
+            // of the tile, (p, q) = (0, d) at step 0, overwrites it
+            const uint32_t acc = (step > 0 || p > 0) ? 1u : 0u;
+            mma_i8(tmem + (uint32_t)((p + q) * QBN), sw32_desc(a0 + p * A_SLICE), sw32_desc(b0 + q * B_SLICE), acc);
+          }
+        tc_commit(empty0 + 8 * st);
+      }
+      tc_commit(done_bar);
+    }
+  } else {
+    // ------------------------------------------------------ epilogue (warps 0-3: rows 32 w .. 32 w + 31)
+    const bool have = __all_sync(0xffffffffu, nsteps > 0 && mbar_wait(done_bar, 0, abort_flag));
+    tc_fence_after();
+    const int row = m0 + 32 * warp + lane;
+    const bool rowok = row < P.M;
+    const int er = rowok ? max(P.eA[row], EXP_NONE) : 0;
+    const bool lower = P.cflags & GC_LOWER;
+    const bool mirror = P.cflags & GC_MIRROR;
+    double* C = P.C;
+#pragma unroll 1
+    for (int c = 0; c < QBN / 32; ++c) {
+      const int col0 = n0 + 32 * c;
+      double v[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = 0.0;
+      if (have) {
+#pragma unroll 1
+        for (int d = OZ_S - 1; d >= 0; --d) {
+          int acc[32];
+          tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * QBN + 32 * c), acc);
+          const double sc = ldexp(1.0, -7 * (d + 2));
+#pragma unroll
+          for (int j = 0; j < 32; ++j) v[j] += sc * (double)acc[j];
+        }
+      }
+      if (!rowok || col0 >= P.N || (lower && col0 > row)) continue;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const int col = col0 + j;
+        if (col >= P.N || (lower && col > row)) continue;
+        double x = ldexp(v[j], er + max(P.fB[col], EXP_NONE));
+        double* dst = C + (size_t)row * P.ldc + col;
+        if (P.beta != 0.0) x += P.beta * *dst;
+        *dst = x;
+        if (mirror && col < row) C[(size_t)col * P.ldc + row] = x;
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 5) {
+    tc_fence_after();
+    if (nsteps > 0 && lane == 0) mbar_wait(done_bar, 0, abort_flag);
+    __syncwarp();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)TMEM_COLS)
+                 : "memory");
+  }
+}
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct OpPlan {
+  const double* P;
+  int ld, rows, K, kcontig, RB, KT;
+  double alpha;
+  int* exps;
+  int8_t* out;
+};
+
+}  // namespace
+
+int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int* abort_flag, void* ws,
+                   size_t ws_bytes, size_t* ws_needed) {
+  // workspace: per problem the exponents of its rows and columns, per segment
+  // the digit images of both operands
+  size_t need = 0;
+  for (const GemmProb& p : probs) {
+    if (p.M <= 0 || p.N <= 0) continue;
+    need += align256((size_t)p.M * 4) + align256((size_t)p.N * 4);
+    for (int s = 0; s < p.nseg; ++s) {
+      const size_t KT = (size_t)(p.seg[s].K + QBK - 1) / QBK;
+      const size_t RBa = 2 * (size_t)((p.M + QBM - 1) / QBM), RBb = (size_t)(p.N + QBN - 1) / QBN;
+      need += align256(OZ_S * KT * RBa * IMG) + align256(OZ_S * KT * RBb * IMG);
+      if (p.seg[s].K > 19000) return cudaErrorInvalidValue;  // INT32 accumulation bound
+    }
+  }
+  if (ws_needed) *ws_needed = need;
+  if (!ws) return cudaSuccess;
+  if (ws_bytes < need || !abort_flag) return cudaErrorInvalidValue;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(gemm_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)QSMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  uint8_t* w = static_cast<uint8_t*>(ws);
+  std::vector<OpPlan> ops;
+  std::vector<QProb> qp;
+  for (const GemmProb& p : probs) {
+    if (p.M <= 0 || p.N <= 0) continue;
+    QProb q{};
+    q.C = p.C;
+    q.ldc = p.ldc;
+    q.M = p.M;
+    q.N = p.N;
+    q.beta = p.beta;
+    q.cflags = p.cflags;
+    q.nseg = p.nseg;
+    q.tmn = (p.M + QBM - 1) / QBM;
+    q.tnn = (p.N + QBN - 1) / QBN;
+    if ((p.cflags & GC_LOWER) && p.M != p.N) return cudaErrorInvalidValue;
+    int* eA = reinterpret_cast<int*>(w);
+    w += align256((size_t)p.M * 4);
+    int* fB = reinterpret_cast<int*>(w);
+    w += align256((size_t)p.N * 4);
+    q.eA = eA;
+    q.fB = fB;
+    // row / column maxima combine by atomicMax from the lowest int
+    if (cudaMemsetAsync(eA, 0x80, (size_t)p.M * 4, stream) != cudaSuccess) return cudaErrorUnknown;
+    if (cudaMemsetAsync(fB, 0x80, (size_t)p.N * 4, stream) != cudaSuccess) return cudaErrorUnknown;
+    for (int s = 0; s < p.nseg; ++s) {
+      const GemmSeg& g = p.seg[s];
+      const int KT = (g.K + QBK - 1) / QBK;
+      const int RBa = 2 * q.tmn, RBb = q.tnn;
+      int8_t* da = reinterpret_cast<int8_t*>(w);
+      w += align256((size_t)OZ_S * KT * RBa * IMG);
+      int8_t* db = reinterpret_cast<int8_t*>(w);
+      w += align256((size_t)OZ_S * KT * RBb * IMG);
+      ops.push_back({g.A, g.lda, p.M, g.K, (g.flags & GF_A_T) ? 0 : 1, RBa, KT, g.alpha, eA, da});
+      ops.push_back({g.B, g.ldb, p.N, g.K, (g.flags & GF_B_KN) ? 0 : 1, RBb, KT, 1.0, fB, db});
+      q.seg[s] = QSeg{da, db, KT, RBa, RBb, g.flags, g.K};
+    }
+    qp.push_back(q);
+  }
+  // exponents, then digits (every exponent of a problem is final before its
+  // operands are cut)
+  for (int pass = 0; pass < 2; ++pass) {
+    size_t i = 0;
+    while (i < ops.size()) {
+      SliceBatch sb;
+      std::memset(&sb, 0, sizeof(sb));
+      int units = 0, chunks = 0;
+      for (; i < ops.size() && sb.count < SLICE_MAXJ; ++i) {
+        const OpPlan& o = ops[i];
+        SliceJob& J = sb.job[sb.count++];
+        J.P = o.P;
+        J.alpha = o.alpha;
+        J.exps = o.exps;
+        J.out = o.out;
+        J.ld = o.ld;
+        J.rows = o.rows;
+        J.K = o.K;
+        J.kcontig = o.kcontig;
+        J.RB = o.RB;
+        J.KT = o.KT;
+        J.unit_start = units;
+        J.chunk_start = chunks;
+        units += ((o.rows + 31) / 32) * std::max(1, (o.K + EXP_KCHUNK - 1) / EXP_KCHUNK);
+        chunks += o.RB * 64 * 2 * o.KT;
+      }
+      sb.units = units;
+      sb.chunks = chunks;
+      bta::ProfScope _ps(bta::PROF_GEMM, stream);
+      if (pass == 0) {
+        const int grid = std::max(1, std::min((units * 32 + 255) / 256, 148 * 16));
+        slice_exp_kernel<<<grid, 256, 0, stream>>>(sb);
+      } else {
+        const int grid = std::max(1, std::min((chunks + 255) / 256, 148 * 16));
+        slice_kernel<<<grid, 256, 0, stream>>>(sb);
+      }
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+    }
+  }
+  size_t i = 0;
+  while (i < qp.size()) {
+    QBatch b;
+    std::memset(&b, 0, sizeof(b));
+    int total = 0;
+    for (; i < qp.size() && b.count < QMAXP; ++i) {
+      const QProb& q = qp[i];
+      int tiles = 0;
+      if (q.cflags & GC_LOWER) {
+        for (int tm = 0; tm < q.tmn; ++tm) tiles += std::min(2 * tm + 2, q.tnn);
+      } else {
+        tiles = q.tmn * q.tnn;
+      }
+      b.p[b.count] = q;
+      b.tile_start[b.count] = total;
+      total += tiles;
+      b.count++;
+    }
+    b.tile_start[b.count] = total;
+    {
+      bta::ProfScope _ps(bta::PROF_GEMM, stream);
+      gemm_i8_kernel<<<total, QTHREADS, QSMEM_BYTES, stream>>>(b, abort_flag);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+}  // namespace bta

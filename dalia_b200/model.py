@@ -113,7 +113,7 @@ def selinv_gemm_flops(n, b, a):
     return (n - 1) * (4 * b ** 3 + 6 * a * b ** 2) + n * (b ** 3 / 3 + 4 * a * b ** 2 + 4 * a * a * b)
 
 
-_PRECISIONS = {"fp64": _lib.BTA_PREC_FP64, "tf32x3": _lib.BTA_PREC_TF32X3}
+_PRECISIONS = {"fp64": _lib.BTA_PREC_FP64, "tf32x3": _lib.BTA_PREC_TF32X3, "i8slice": _lib.BTA_PREC_I8SLICE}
 
 
 class BTAMatrix:
@@ -179,9 +179,10 @@ class SpatioTemporalModel:
     def __init__(self, prob, priors=None, fe_prec=1e-3, eps_gradient_f=1e-3, eps_inner_iteration=1e-3,
                  inner_iteration_max_iter=50, device=None, selinv_precision="fp64", mixed_tolerance=1e-8):
         """selinv_precision: arithmetic of the selected inversions behind the
-        adjoint gradient, "fp64" or "tf32x3" (FP32-class block products on the
-        tcgen05 tensor cores; factorisations, log-determinants and solves stay
-        FP64).  Every adjoint evaluation checks its selected inverses through
+        adjoint gradient: "fp64", "tf32x3" (FP32-class block products on the
+        tcgen05 tensor cores) or "i8slice" (8-bit digit products accumulated
+        exactly in INT32 on the tensor cores, ~1e-10 relative); the
+        factorisations, log-determinants and solves stay FP64.  Every adjoint evaluation checks its selected inverses through
         the identity <S, Q> = dim(Q) over the BTA pattern; a "tf32x3" point
         whose relative residual exceeds mixed_tolerance is recomputed in FP64.
         The residuals of the last evaluation are in ``last_check``."""
@@ -632,7 +633,9 @@ class SpatioTemporalModel:
         f2, g2 = self.objective_adjoint_batched([thetas[j] for j in bad], precision="fp64")
         for j, f, g, c in zip(bad, f2, g2, self.last_check):
             fs[j], grads[j] = f, g
-            checks[j] = dict(c, fallback=True)
+            # the reduced-precision residuals that triggered the recomputation stay reported
+            checks[j] = dict(checks[j], fallback=True, fp64_residual_c=c["residual_c"],
+                             fp64_residual_p=c["residual_p"])
         self.last_check = checks
         return fs, grads
 

@@ -82,11 +82,17 @@ int bta_pobtasi_batched(bta_handle_t h, int count, const int64_t* n, const int64
  * BTA_PREC_FP64 -- FP64 on the DMMA tensor pipe (the default everywhere);
  * BTA_PREC_TF32X3 -- FP32-class: every FP64 operand is split into two TF32
  * values and the products are accumulated in FP32 on the tcgen05 tensor
- * cores (relative error of the selected inverse ~1e-7).  The factor, the
- * diagonal-block inverses and all storage stay FP64.
+ * cores (relative error of the selected inverse ~1e-5, growing with b: the
+ * tensor cores accumulate FP32 with truncation);
+ * BTA_PREC_I8SLICE -- every operand row / column scaled by a power of two and
+ * cut into seven signed 7-bit digits; the digit products are accumulated
+ * exactly in INT32 on the tcgen05 tensor cores (kind::i8) and recombined in
+ * FP64 (relative error ~1e-14 against sum |a||b|; block sizes up to 19000).
+ * The factor, the diagonal-block inverses and all storage stay FP64.
  */
 #define BTA_PREC_FP64 0
 #define BTA_PREC_TF32X3 1
+#define BTA_PREC_I8SLICE 2
 int bta_pobtasi_batched_ex(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
                            double* const* D, double* const* L, double* const* Ab, double* const* T,
                            int precision);

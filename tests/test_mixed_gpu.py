@@ -9,7 +9,12 @@ data, ~1e-5 for a selected inverse); the GEMM is held to 5e-6 and the
 selected inverse to 3e-5 (norm-wise).  That is not enough for the adjoint
 gradient's 1e-6 bar, so the default tolerance of the <S, Q> = N check
 sends TF32x3 points back to FP64, whose results must then be reproduced
-exactly."""
+exactly.
+
+The 8-bit-slice arithmetic (BTA_PREC_I8SLICE) accumulates exactly; its error
+is the digit truncation, ~1e-9 relative per product (2e-8 after the selected
+inversion's recurrence), so it is held to 1e-8 on the GEMM, 1e-7 on the
+selected inverse and to the gradient bar of 1e-6."""
 import ctypes
 
 import numpy as np
@@ -129,7 +134,7 @@ def test_tf32x3_adjoint_check_and_fallback(name):
     # default tolerance: the point is recomputed in FP64
     md = SpatioTemporalModel(prob, selinv_precision="tf32x3")
     fd, gd = md.objective_adjoint(th)
-    assert md.last_check[0]["fallback"]
+    assert md.last_check[0]["fallback"] and md.last_check[0]["precision"] == "tf32x3"
     assert abs(fd - f64) < 1e-12 * abs(f64) and rel(gd, g64) < 1e-10
 
 
@@ -145,3 +150,74 @@ def test_mixed_fallback_recomputes_in_fp64():
     assert mm.last_check[0]["fallback"]
     assert abs(fm - f64) < 1e-12 * abs(f64)
     assert rel(gm, g64) < 1e-10
+
+
+@pytest.mark.parametrize("case", GEMM_CASES)
+def test_gemm_i8slice_matches_numpy(case):
+    from dalia_b200 import _lib
+
+    lib = _lib.load()
+    h = _lib.handle()
+    M, N, K, at, bkn, lower, mirror, alpha, beta = case
+    for rep in range(2):
+        got, exp = _gemm(lib, h, _lib.BTA_PREC_I8SLICE, *case, seed=M + N + K + rep)
+        assert rel(got, exp) < 1e-8
+
+
+@pytest.mark.parametrize("n,b,a", [(3, 200, 6), (4, 129, 0), (2, 300, 70)])
+def test_selinv_i8slice_matches_oracle(n, b, a):
+    import torch
+
+    from dalia_b200 import _lib
+
+    lib = _lib.load()
+    h = _lib.handle()
+    rng = np.random.default_rng(7 * n + b + a)
+    D, L, Ab, T = bta_ref.random_bta(n, b, a, rng)
+    ref = [x.copy() for x in (D, L, Ab, T)]
+    bta_ref.pobtaf(*ref)
+    bta_ref.pobtasi(*ref)
+    d = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (D, L, Ab, T)]
+    arr = lambda t: (ctypes.c_void_p * 1)(t.data_ptr() if t.numel() else None)
+    i64 = lambda v: (ctypes.c_int64 * 1)(v)
+    args = (h.bind_stream(), 1, i64(n), i64(b), i64(a), arr(d[0]), arr(d[1]), arr(d[2]), arr(d[3]))
+    _lib.check(lib.bta_pobtaf_batched(*args, None), "pobtaf")
+    _lib.check(lib.bta_pobtasi_batched_ex(*args, _lib.BTA_PREC_I8SLICE), "pobtasi")
+    st = ctypes.c_int64(0)
+    _lib.check(lib.bta_get_status(h.bind_stream(), ctypes.byref(st)), "status")
+    got = [t.cpu().numpy() for t in d]
+    assert rel(got[0], ref[0]) < 1e-7
+    if n > 1:
+        assert rel(got[1], ref[1]) < 1e-7
+    if a:
+        assert rel(got[2], ref[2]) < 1e-7 and rel(got[3], ref[3]) < 1e-7
+
+
+@pytest.mark.parametrize("name", ["gst_300x10", "pst_150x6"])
+def test_i8slice_adjoint_meets_the_gradient_bar(name):
+    from dalia_b200.model import SpatioTemporalModel
+
+    g = load(name)
+    prob = problem(g)
+    th = g["theta"]
+    f64, g64 = SpatioTemporalModel(prob).objective_adjoint(th)
+    m = SpatioTemporalModel(prob, selinv_precision="i8slice")
+    f, gr = m.objective_adjoint(th)
+    chk = m.last_check[0]
+    assert chk["precision"] == "i8slice" and not chk["fallback"]
+    assert abs(f - f64) < 1e-12 * abs(f64)
+    assert rel(gr, g64) < 1e-6
+
+
+def test_i8slice_coregional_adjoint():
+    from golden_util import coreg_problem
+
+    from dalia_b200.coregional import CoregionalModel
+
+    g = load("gst_coreg3_small")
+    prob = coreg_problem(g)
+    f64, g64 = CoregionalModel(prob).objective_adjoint(g["theta"])
+    m = CoregionalModel(prob, selinv_precision="i8slice")
+    f, gr = m.objective_adjoint(g["theta"])
+    assert not m.last_check[0]["fallback"]
+    assert abs(f - f64) < 1e-12 * max(1.0, abs(f64)) and rel(gr, g64) < 1e-6
