@@ -594,6 +594,49 @@ class SpatioTemporalModel:
             fv[idx] = self.evaluate_f_batched([tm[:, i] for i in idx])
         return fv[0], (fv[1:1 + d] - fv[d + 1:nf]) / (2 * self.eps)
 
+    def hessian_fd(self, theta, eps_hessian_f=5e-3, max_points=16):
+        """Finite-difference Hessian of f (``DALIA._evaluate_hessian_f``,
+        ``dalia.py:767-910``): f at theta, at theta +- eps e_i and at
+        theta +- eps e_i +- eps e_j (i < j), 1 + 2d + 2d(d-1) points.  Gaussian
+        likelihoods evaluate the points in batches of max_points; a Poisson
+        likelihood evaluates them one by one in the reference's order, because
+        each Newton iteration starts from the previous point's mode."""
+        theta = np.asarray(theta, dtype=np.float64)
+        d = theta.size
+        h = float(eps_hessian_f)
+        E = h * np.eye(d)
+        pts = [theta.copy()]
+        slot_of = {}
+        for k in range(d * d):
+            i, j = divmod(k, d)
+            if i == j:
+                slot_of[("+", i)] = len(pts)
+                pts.append(theta + E[i])
+                slot_of[("-", i)] = len(pts)
+                pts.append(theta - E[i])
+            elif i < j:
+                for si, sj in ((1, 1), (1, -1), (-1, 1), (-1, -1)):
+                    slot_of[(i, j, si, sj)] = len(pts)
+                    pts.append(theta + si * E[i] + sj * E[j])
+        if self.gaussian:
+            fv = []
+            for c0 in range(0, len(pts), max_points):
+                fv += self.evaluate_f_batched(pts[c0:c0 + max_points])
+        else:
+            fv = [self.evaluate_f(p) for p in pts]
+        H = np.zeros((d, d))
+        for i in range(d):
+            H[i, i] = (fv[slot_of[("+", i)]] - 2 * fv[0] + fv[slot_of[("-", i)]]) / h ** 2
+            for j in range(i + 1, d):
+                H[i, j] = H[j, i] = (fv[slot_of[(i, j, 1, 1)]] - fv[slot_of[(i, j, 1, -1)]]
+                                     - fv[slot_of[(i, j, -1, 1)]] + fv[slot_of[(i, j, -1, -1)]]) / (4 * h * h)
+        return H
+
+    def covariance_theta(self, theta, eps_hessian_f=5e-3):
+        """Covariance of the hyperparameters, the inverse of the FD Hessian
+        (``DALIA.compute_covariance_hp``, ``dalia.py:747-765``)."""
+        return np.linalg.inv(self.hessian_fd(theta, eps_hessian_f))
+
     def _dcoef(self, theta, k):
         th = np.asarray(theta, dtype=np.complex128).copy()
         th[k] += 1j * _CSTEP

@@ -334,3 +334,50 @@ def dense_adjoint_gradient_poisson(model: OracleModel, theta):
         grad[k] = (0.5 * xs @ dQc @ xs + 0.5 * np.sum(Sc * dQc) - 0.5 * np.sum(Sp * dQ) + u @ dQc @ xs
                    - _cstep(lambda th: _log_prior_complex(model, th), theta, k))
     return grad
+
+
+def hessian_points(theta, eps):
+    """The evaluation points of DALIA._evaluate_hessian_f in its order
+    (``src/dalia/core/dalia.py:767-851``): theta, then for k = i*d + j:
+    i == j -> theta +- eps e_i; i < j -> theta +eps_i +eps_j, +eps_i -eps_j,
+    -eps_i +eps_j, -eps_i -eps_j.  Returns (points, combine) where
+    combine(f_values) -> the Hessian (``:858-899``)."""
+    theta = np.asarray(theta, dtype=np.float64)
+    d = theta.size
+    E = eps * np.eye(d)
+    pts, keys = [theta.copy()], [("c",)]
+    for k in range(d * d):
+        i, j = divmod(k, d)
+        if i == j:
+            pts += [theta + E[i], theta - E[i]]
+            keys += [("ii+", i), ("ii-", i)]
+        elif i < j:
+            for si, sj, tag in ((1, 1, 0), (1, -1, 1), (-1, 1, 2), (-1, -1, 3)):
+                pts.append(theta + si * E[i] + sj * E[j])
+                keys.append(("ij", i, j, tag))
+
+    def combine(fv):
+        f0 = fv[0]
+        fii = np.zeros((2, d))
+        fij = np.zeros((4, d, d))
+        for key, f in zip(keys, fv):
+            if key[0] == "ii+":
+                fii[0, key[1]] = f
+            elif key[0] == "ii-":
+                fii[1, key[1]] = f
+            elif key[0] == "ij":
+                fij[key[3], key[1], key[2]] = f
+        H = np.zeros((d, d))
+        for i in range(d):
+            H[i, i] = (fii[0, i] - 2 * f0 + fii[1, i]) / eps ** 2
+            for j in range(i + 1, d):
+                H[i, j] = H[j, i] = (fij[0, i, j] - fij[1, i, j] - fij[2, i, j] + fij[3, i, j]) / (4 * eps * eps)
+        return H
+
+    return pts, combine
+
+
+def hessian_fd(evaluate_f, theta, eps=5e-3):
+    """FD Hessian with f evaluated point by point in the reference's order."""
+    pts, combine = hessian_points(theta, eps)
+    return combine([evaluate_f(p) for p in pts])

@@ -64,7 +64,16 @@ def checksums(prob):
     return out
 
 
-def main(ref_root: str, only=None) -> None:
+def _save_hessian(name, th, dal):
+    """hess_<name>.npz: DALIA._evaluate_hessian_f at theta (Serinv path,
+    default eps_hessian_f = 5e-3, points evaluated in the reference's order)."""
+    h = dal._evaluate_hessian_f(th.copy())
+    np.savez_compressed(os.path.join(HERE, f"hess_{name}.npz"), theta=th, hess=np.asarray(h),
+                        eps_hessian_f=np.array(dal.eps_hessian_f))
+    print(f"hess_{name}: diag={np.diag(np.asarray(h))}", flush=True)
+
+
+def main(ref_root: str, only=None, hessian=False) -> None:
     os.environ.setdefault("ARRAY_MODULE", "numpy")
     sys.path.insert(0, REPO)
     sys.path.insert(0, os.path.join(ref_root, "src"))
@@ -140,9 +149,13 @@ def main(ref_root: str, only=None) -> None:
         for k, v in checksums(prob).items():
             out[f"chk_{k}"] = v
 
+        th = np.asarray(theta, dtype=np.float64)
+        if hessian:
+            _save_hessian(name, th, build("serinv")[1])
+            continue
+
         # --- dense solver: exact reference numbers
         model, dal = build("dense")
-        th = np.asarray(theta, dtype=np.float64)
         model.theta[:] = th
         Qp = model.construct_Q_prior().tocoo()
         eta0 = np.zeros_like(model.y)
@@ -196,7 +209,7 @@ def coreg_checksums(prob):
     return out
 
 
-def main_coregional(ref_root: str, only=None) -> None:
+def main_coregional(ref_root: str, only=None, hessian=False) -> None:
     """Coregional fixtures: the reference's ``CoregionalModel`` built from one
     ``Model`` per variate (Gaussian priors as in its coregional examples),
     driven through ``DALIA._objective_function`` with the dense and the
@@ -257,6 +270,9 @@ def main_coregional(ref_root: str, only=None) -> None:
             dal.iter = 0
             return model, dal
 
+        if hessian:
+            _save_hessian(name, th, build("serinv")[1])
+            continue
         out = {"theta": th, "shape": np.array([ns, nt, nv, nb, no, seed])}
         for k, v in coreg_checksums(prob).items():
             out[f"chk_{k}"] = v
@@ -276,10 +292,12 @@ def main_coregional(ref_root: str, only=None) -> None:
 
 
 if __name__ == "__main__":
-    # usage: make_golden.py [REF_ROOT [CASE ...]]
+    # usage: make_golden.py [REF_ROOT [--hessian] [CASE ...]]
+    #   --hessian writes hess_<CASE>.npz (the reference's FD Hessian) instead
     _root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DALIA_REF", "/root/reference")
-    _only = sys.argv[2:]
+    _hess = "--hessian" in sys.argv[2:]
+    _only = [a for a in sys.argv[2:] if a != "--hessian"]
     if not _only or any(c in CASES for c in _only):
-        main(_root, [c for c in _only if c in CASES])
+        main(_root, [c for c in _only if c in CASES], hessian=_hess)
     if not _only or any(c in COREG_CASES for c in _only):
-        main_coregional(_root, [c for c in _only if c in COREG_CASES])
+        main_coregional(_root, [c for c in _only if c in COREG_CASES], hessian=_hess)
