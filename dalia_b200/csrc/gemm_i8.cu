@@ -535,7 +535,7 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
       }
       sb.units = units;
       sb.chunks = chunks;
-      bta::ProfScope _ps(bta::PROF_GEMM, stream);
+      bta::ProfScope _ps(bta::PROF_SLICE, stream);
       if (pass == 0) {
         const int grid = std::max(1, std::min((units * 32 + 255) / 256, 148 * 16));
         slice_exp_kernel<<<grid, 256, 0, stream>>>(sb);

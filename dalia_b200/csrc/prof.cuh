@@ -7,7 +7,16 @@
 
 namespace bta {
 
-enum ProfCat : int { PROF_PANEL = 0, PROF_GEMM = 1, PROF_SWEEP = 2, PROF_TRTRI = 3, PROF_OTHER = 4, PROF_NCAT = 8 };
+// PROF_SLICE: the digit pre-pass of the 8-bit-slice GEMM
+enum ProfCat : int {
+  PROF_PANEL = 0,
+  PROF_GEMM = 1,
+  PROF_SWEEP = 2,
+  PROF_TRTRI = 3,
+  PROF_OTHER = 4,
+  PROF_SLICE = 5,
+  PROF_NCAT = 8
+};
 
 void prof_begin(int cat, cudaStream_t s, cudaEvent_t* ev);
 void prof_end(int cat, cudaStream_t s, cudaEvent_t ev);
