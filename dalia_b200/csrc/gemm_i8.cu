@@ -220,12 +220,26 @@ __global__ void __launch_bounds__(256) slice_kernel(const __grid_constant__ Slic
     for (int p = 0; p < OZ_S; ++p)
 #pragma unroll
       for (int i = 0; i < 4; ++i) w[p][i] = 0u;
+    double xs[16];
+    if (J.kcontig && r < J.rows && k0 + 15 < J.K && ((J.ld & 1) == 0) &&
+        ((reinterpret_cast<uintptr_t>(J.P) & 15) == 0)) {
+      const double2* src = reinterpret_cast<const double2*>(J.P + (size_t)r * J.ld + k0);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const double2 v = src[j];
+        xs[2 * j] = v.x;
+        xs[2 * j + 1] = v.y;
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int k = k0 + j;
+        xs[j] = (r < J.rows && k < J.K) ? J.P[J.kcontig ? (size_t)r * J.ld + k : (size_t)k * J.ld + r] : 0.0;
+      }
+    }
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-      const int k = k0 + j;
-      double x = 0.0;
-      if (r < J.rows && k < J.K) x = J.P[J.kcontig ? (size_t)r * J.ld + k : (size_t)k * J.ld + r];
-      x *= J.alpha;
+      const double x = xs[j] * J.alpha;
       const unsigned long long U = __double2ull_rz(ldexp(fabs(x), 7 * OZ_S - e));
       const bool neg = x < 0.0;
 #pragma unroll
