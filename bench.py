@@ -63,6 +63,36 @@ def dist_info():
         os.environ.get("LOCAL_RANK", "0"))
 
 
+# ------------------------------------------------------------ replicas
+def replica_theta(theta, rank):
+    """Each rank evaluates its own theta points (independent replicas, no
+    collective on the data path)."""
+    return np.asarray(theta, dtype=np.float64) + 1e-3 * rank
+
+
+def step_points(theta, step, K):
+    """The K candidates of one step; theta moves between steps as in an
+    optimiser, so warm starts of a Newton iteration see a new point."""
+    base = theta + 0.005 * (step % 4)
+    return [base + 1e-3 * j for j in range(K)]
+
+
+def max_over_ranks(t, world, device=None):
+    """Slowest rank's time (the job ends when it does)."""
+    if world <= 1:
+        return float(t)
+    import torch
+
+    tt = torch.tensor([float(t)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def job_rate(units_per_rank, world, t_max):
+    """Whole-job throughput: the units all ranks processed / the slowest time."""
+    return units_per_rank * world / t_max
+
+
 # ----------------------------------------------------------------- CPU port
 def cpu_sample(workload, nt_sample, reps=1):
     """Time one f(theta) of the CPU oracle on the workload truncated to
@@ -213,7 +243,7 @@ def run_ours(args):
     model = (CoregionalModel if coreg else SpatioTemporalModel)(prob, device=dev, selinv_precision=args.precision)
     n, b, a = model.nt, model.b, model.nb
     # replicas evaluate different theta points (a line-search batch)
-    theta = np.asarray(cfg["theta"], dtype=np.float64) + 1e-3 * rank
+    theta = replica_theta(cfg["theta"], rank)
 
     peak = measured_fp64_peak(torch, dev)
 
@@ -225,10 +255,7 @@ def run_ours(args):
     K = max(1, args.batch)
 
     def step_thetas(step):
-        # theta moves between steps as in an optimiser (warm starts of the
-        # Newton iteration see a new point every step); K candidates per step
-        base = theta + 0.005 * (step % 4)
-        return [base + 1e-3 * j for j in range(K)]
+        return step_points(theta, step, K)
 
     # ---- warm-up
     nwarm = max(args.warmup, 3)
@@ -262,12 +289,8 @@ def run_ours(args):
     cnt_cat = (__import__("ctypes").c_longlong * 8)()
     lib.bta_prof_read(ms_cat, cnt_cat)
     clocks = clock.stop()
-    t_dev = e0.elapsed_time(e1) * 1e-3
-    if world > 1:
-        tt = torch.tensor([t_dev], device=dev)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_dev = float(tt.item())
-    value = K * args.steps * world / t_dev
+    t_dev = max_over_ranks(e0.elapsed_time(e1) * 1e-3, world, dev)
+    value = job_rate(K * args.steps, world, t_dev)
 
     # ---- single-point adjoint latency
     barrier()
@@ -286,12 +309,8 @@ def run_ours(args):
         th_host = [np.array(t) for t in step_thetas(nwarm + args.steps + s)]  # host buffers
         fs, gs = model.objective_adjoint_batched(th_host)
     torch.cuda.synchronize()
-    t_e2e = time.perf_counter() - t0
-    if world > 1:
-        tt = torch.tensor([t_e2e], device=dev)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_e2e = float(tt.item())
-    e2e = K * args.steps * world / t_e2e
+    t_e2e = max_over_ranks(time.perf_counter() - t0, world, dev)
+    e2e = job_rate(K * args.steps, world, t_e2e)
     f, g = fs[0], gs[0]
     coef_bytes = model.slots[0].coef_host[0].numel() * 8
     h2d = K * 2 * coef_bytes
