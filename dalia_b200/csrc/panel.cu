@@ -102,6 +102,92 @@ __device__ __forceinline__ TileRef prev_tile_of(const PanelInst& I, int p, int c
   return t;
 }
 
+// The previous block column's Schur update streams whole 64-row blocks of
+// Lprev / Abprev through a ring of 16-wide k-slabs, so loading slab s+2
+// overlaps the DMMA work on slab s (it needs no dependency waits: that column
+// is final before the launch).
+constexpr int PK = 16;
+constexpr int PSK = PK + 4;  // slab row stride: conflict-light DMMA fragment loads
+constexpr int PST = 3;
+constexpr int PSLAB = T * PSK;
+static_assert(2 * PST * PSLAB <= 2 * T * SG, "slab ring exceeds the two tile buffers");
+
+// 64 x 16 slab of a row block at g (row stride ld): rows < rows and columns
+// k0 .. k0+15 < kmax, zero-filled elsewhere.
+__device__ __forceinline__ void load_slab(double* s, const double* g, int ld, int rows, int k0, int kmax, bool vec,
+                                          int tid) {
+#pragma unroll
+  for (int j = 0; j < (T * PK / 2) / THREADS; ++j) {
+    const int c = tid + j * THREADS;
+    const int r = c >> 3, kc = (c & 7) * 2;
+    const int gk = k0 + kc;
+    double* d = s + r * PSK + kc;
+    const bool v0 = r < rows && gk < kmax;
+    const bool v1 = r < rows && gk + 1 < kmax;
+    const double* src = g + (size_t)r * ld + gk;
+    if (vec && v1) {
+      cp_async16(d, src, true);
+    } else {
+      cp_async8(d, v0 ? src : g, v0);
+      cp_async8(d + 1, v1 ? src + 1 : g, v1);
+    }
+  }
+}
+
+__device__ __forceinline__ void mma_slab(const double* X, const double* Y, double (&acc)[2][4][4], int wm, int wn,
+                                         int g, int t) {
+#pragma unroll
+  for (int kk = 0; kk < PK; kk += 4) {
+    double a[2][2], b[4];
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi) {
+      const int r = wm * 32 + mi * 16 + g;
+      a[mi][0] = X[r * PSK + kk + t];
+      a[mi][1] = X[(r + 8) * PSK + kk + t];
+    }
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni) b[ni] = Y[(wn * 32 + ni * 8 + g) * PSK + kk + t];
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) dmma16x8x4(acc[mi][ni], a[mi][0], a[mi][1], b[ni]);
+  }
+}
+
+// acc += Xrow(p) Xrow(r)^T over the full width of the previous block column.
+__device__ void acc_prev_stream(const PanelInst& I, int p, int r, double* smem, double (&acc)[2][4][4], int tid,
+                                int wm, int wn, int g, int t) {
+  const TileRef x0 = prev_tile_of(I, p, 0), y0 = prev_tile_of(I, r, 0);
+  const int ld = I.b, kmax = I.b;
+  const int nslab = (kmax + PK - 1) / PK;
+  const bool vec = ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(x0.ptr) & 15) == 0) &&
+                   ((reinterpret_cast<uintptr_t>(y0.ptr) & 15) == 0);
+  double* As = smem;
+  double* Bs = smem + PST * PSLAB;
+  __syncthreads();  // the tile buffers may still be read by the previous step
+#pragma unroll
+  for (int st = 0; st < PST - 1; ++st) {
+    if (st < nslab) {
+      load_slab(As + st * PSLAB, x0.ptr, ld, x0.rows, st * PK, kmax, vec, tid);
+      load_slab(Bs + st * PSLAB, y0.ptr, ld, y0.rows, st * PK, kmax, vec, tid);
+    }
+    cp_async_commit();
+  }
+  for (int s = 0; s < nslab; ++s) {
+    cp_async_wait<PST - 2>();
+    __syncthreads();
+    const int nx = s + PST - 1;
+    if (nx < nslab) {
+      load_slab(As + (nx % PST) * PSLAB, x0.ptr, ld, x0.rows, nx * PK, kmax, vec, tid);
+      load_slab(Bs + (nx % PST) * PSLAB, y0.ptr, ld, y0.rows, nx * PK, kmax, vec, tid);
+    }
+    cp_async_commit();
+    mma_slab(As + (s % PST) * PSLAB, Bs + (s % PST) * PSLAB, acc, wm, wn, g, t);
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+}
+
 // acc += X Y^T for two global tiles (staged through the two smem buffers).
 __device__ __forceinline__ void acc_pair(const TileRef& x, const TileRef& y, double* bufA, double* bufL, int ld,
                                          double (&acc)[2][4][4], int tid, int wm, int wn, int g, int t) {
@@ -285,10 +371,7 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
     }
     if (I.Lprev != nullptr) {
       const TileRef yp0 = prev_tile_of(I, r, 0);
-      if (prev_tile_of(I, p, 0).rows > 0 && yp0.rows > 0) {
-        for (int k = 0; k < nq; ++k) acc_pair(prev_tile_of(I, p, k), prev_tile_of(I, r, k), bufA, bufL, ld, acc, tid,
-                                              wm, wn, g, t);
-      }
+      if (prev_tile_of(I, p, 0).rows > 0 && yp0.rows > 0) acc_prev_stream(I, p, r, bufA, acc, tid, wm, wn, g, t);
     }
     // zero the mirrored strictly-upper tile (r, p) of the diagonal block
     if (p < nq && p > r) {
