@@ -13,6 +13,93 @@ namespace {
 using namespace tile;
 constexpr size_t TRTRI_SMEM = size_t(3) * T * SG * sizeof(double);
 
+// Slab ring of the column substitution: A = 64 rows x 16 k of a row block of
+// the factor (k-contiguous, stride TSK), B = 16 k x 64 columns of the output
+// (n-contiguous, stride TSN), three stages in the As / Bs buffers.
+constexpr int TK = 16, TSK = TK + 4, TSN = T + 4, TST = 3;
+constexpr int TA_SLAB = T * TSK, TB_SLAB = TK * TSN;
+static_assert(TST * (TA_SLAB + TB_SLAB) <= 2 * T * SG, "slab ring exceeds As + Bs");
+
+__device__ __forceinline__ void trtri_load(double* As, double* Bs, const double* Arow, int rows, const double* Bcol,
+                                           int cols, int k0, int kend, int ld, int tid) {
+  const bool va = ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(Arow) & 15) == 0);
+  const bool vb = ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(Bcol) & 15) == 0);
+#pragma unroll
+  for (int j = 0; j < (T * TK / 2) / THREADS; ++j) {
+    const int q = tid + j * THREADS;
+    // A: row r, k pair kc
+    {
+      const int r = q >> 3, kc = (q & 7) * 2, gk = k0 + kc;
+      double* d = As + r * TSK + kc;
+      const bool v0 = r < rows && gk < kend, v1 = r < rows && gk + 1 < kend;
+      const double* src = Arow + (size_t)r * ld + gk;
+      if (va && v1) {
+        cp_async16(d, src, true);
+      } else {
+        cp_async8(d, v0 ? src : Arow, v0);
+        cp_async8(d + 1, v1 ? src + 1 : Arow, v1);
+      }
+    }
+    // B: k row kr, column pair nc
+    {
+      const int kr = q >> 5, nc = (q & 31) * 2, gk = k0 + kr;
+      double* d = Bs + kr * TSN + nc;
+      const bool v0 = gk < kend && nc < cols, v1 = gk < kend && nc + 1 < cols;
+      const double* src = Bcol + (size_t)gk * ld + nc;
+      if (vb && v1) {
+        cp_async16(d, src, true);  // .cg: from L2, where this CTA's earlier rows were written
+      } else {
+        d[0] = v0 ? __ldcg(src) : 0.0;
+        d[1] = v1 ? __ldcg(src + 1) : 0.0;
+      }
+    }
+  }
+}
+
+// acc += A[:, k0:kend] B[k0:kend, :] with A = rows x (.) at Arow, B = (.) x cols
+// at Bcol (both row stride ld), through a 3-stage cp.async ring.
+__device__ void trtri_stream(const double* Arow, int rows, const double* Bcol, int cols, int k0, int kend, int ld,
+                             double* smem, double (&acc)[2][4][4], int tid, int wm, int wn, int g, int t) {
+  double* As = smem;
+  double* Bs = smem + TST * TA_SLAB;
+  const int nslab = (kend - k0 + TK - 1) / TK;
+  __syncthreads();
+#pragma unroll
+  for (int st = 0; st < TST - 1; ++st) {
+    if (st < nslab) trtri_load(As + st * TA_SLAB, Bs + st * TB_SLAB, Arow, rows, Bcol, cols, k0 + st * TK, kend, ld, tid);
+    cp_async_commit();
+  }
+  for (int s = 0; s < nslab; ++s) {
+    cp_async_wait<TST - 2>();
+    __syncthreads();
+    const int nx = s + TST - 1;
+    if (nx < nslab)
+      trtri_load(As + (nx % TST) * TA_SLAB, Bs + (nx % TST) * TB_SLAB, Arow, rows, Bcol, cols, k0 + nx * TK, kend,
+                 ld, tid);
+    cp_async_commit();
+    const double* X = As + (s % TST) * TA_SLAB;
+    const double* Y = Bs + (s % TST) * TB_SLAB;
+#pragma unroll
+    for (int kk = 0; kk < TK; kk += 4) {
+      double a[2][2], bb[4];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi) {
+        const int r = wm * 32 + mi * 16 + g;
+        a[mi][0] = X[r * TSK + kk + t];
+        a[mi][1] = X[(r + 8) * TSK + kk + t];
+      }
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) bb[ni] = Y[(kk + t) * TSN + wn * 32 + ni * 8 + g];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) dmma16x8x4(acc[mi][ni], a[mi][0], a[mi][1], bb[ni]);
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+}
+
 // One CTA per (block, tile column c): forward substitution down the column,
 //   X[c] = Linv_cc,  X[p] = -Linv_pp * sum_{k=c}^{p-1} L[p][k] X[k]   (p > c).
 // blockIdx.x = c * nblk + block so that the longest columns start first.
@@ -20,7 +107,6 @@ __global__ void __launch_bounds__(THREADS) block_trtri_kernel(const double* D, c
                                                                int nblk, int b, int nq, double* out) {
   extern __shared__ __align__(16) double sm[];
   double* As = sm;
-  double* Bs = sm + T * SG;
   double* Ys = sm + 2 * T * SG;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t = lane & 3;
@@ -51,18 +137,8 @@ __global__ void __launch_bounds__(THREADS) block_trtri_kernel(const double* D, c
     const int rp = min(T, b - p * T);
     double acc[2][4][4];
     zero_acc(acc);
-    for (int k = c; k < p; ++k) {
-      const int wk = min(T, b - k * T);
-      load<SG>(As, Di + (size_t)(p * T) * b + k * T, b, rp, wk, tid);
-      // Bs[n][j] = X[k][j][n]
-      for (int idx = tid; idx < T * T; idx += THREADS) {
-        const int j = idx >> 6, n = idx & 63;
-        Bs[n * SG + j] = (j < wk && n < wc) ? __ldcg(Oi + (size_t)(k * T + j) * b + c * T + n) : 0.0;
-      }
-      __syncthreads();
-      mma_nt(As, Bs, (wk + 3) & ~3, acc, wm, wn, g, t);
-      __syncthreads();
-    }
+    // acc = L[p][c..p-1] X[c..p-1][c], streamed over k in 16-wide slabs
+    trtri_stream(Di + (size_t)(p * T) * b, rp, Oi + c * T, wc, c * T, p * T, b, As, acc, tid, wm, wn, g, t);
     // Ys[n][j] = acc[j][n]
 #pragma unroll
     for (int mi = 0; mi < 2; ++mi)
