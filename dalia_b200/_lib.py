@@ -50,6 +50,11 @@ SIGNATURES = {
                                    _c_void_p, _c_void_p]),
     "bta_pobtasi_batched_ex": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
                                       _c_void_p, _c_void_p, _int]),
+    "bta_block_inverses": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p]),
+    "bta_pobtas_inv_batched": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                      _c_void_p, _c_void_p, _c_void_p, _int]),
+    "bta_pobtasi_batched_v": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                     _c_void_p, _c_void_p, _c_void_p, _int]),
     "bta_gemm": (_int, [_c_void_p, _int, _i64, _i64, _i64, _dbl, _c_void_p, _i64, _int, _c_void_p, _i64, _int,
                         _dbl, _c_void_p, _i64, _int, _int]),
     "bta_pobtasi": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p]),

@@ -434,7 +434,16 @@ int bta_pobtasi_batched(bta_handle_t h, int count, const int64_t* n, const int64
 int bta_pobtasi_batched_ex(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
                            double* const* D, double* const* L, double* const* Ab, double* const* T,
                            int precision) {
+  return bta_pobtasi_batched_v(h, count, n, b, a, D, L, Ab, T, nullptr, precision);
+}
+
+int bta_pobtasi_batched_v(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                          double* const* D, double* const* L, double* const* Ab, double* const* T,
+                          const double* const* V, int precision) {
   if (!h || count < 1 || !n || !b || !a || !D) return BTA_ERR_INVALID;
+  if (V)
+    for (int k = 0; k < count; ++k)
+      if (!V[k]) return BTA_ERR_INVALID;
   if (precision != BTA_PREC_FP64 && precision != BTA_PREC_TF32X3 && precision != BTA_PREC_I8SLICE)
     return BTA_ERR_INVALID;
   // the block products go to the grouped GEMM of the requested arithmetic
@@ -447,8 +456,9 @@ int bta_pobtasi_batched_ex(bta_handle_t h, int count, const int64_t* n, const in
       return BTA_ERR_INVALID;
     const size_t nq = (b[k] + 63) / 64, nqa = (a[k] + 63) / 64;
     const size_t bb = (size_t)b[k] * b[k], ab = (size_t)a[k] * b[k];
-    need += align_up(n[k] * nq * 4096 * 8) + align_up(n[k] * bb * 8) + 2 * align_up(bb * 8) + align_up(ab * 8 + 8) +
-            align_up(nqa * 4096 * 8 + 8) + align_up((size_t)a[k] * a[k] * 8 + 8) + 7 * kAlign;
+    // block inverses (tile inverses + full inverses) only when not supplied
+    need += (V ? 0 : align_up(n[k] * nq * 4096 * 8) + align_up(n[k] * bb * 8)) + 2 * align_up(bb * 8) +
+            align_up(ab * 8 + 8) + align_up(nqa * 4096 * 8 + 8) + align_up((size_t)a[k] * a[k] * 8 + 8) + 7 * kAlign;
     maxn = std::max(maxn, n[k]);
   }
   int rc = ensure_ws(h, need);
@@ -462,8 +472,8 @@ int bta_pobtasi_batched_ex(bta_handle_t h, int count, const int64_t* n, const in
   for (int k = 0; k < count; ++k) {
     const size_t nq = (b[k] + 63) / 64, nqa = (a[k] + 63) / 64;
     const size_t bb = (size_t)b[k] * b[k], ab = (size_t)a[k] * b[k];
-    w[k].tinv = cv.take<double>(n[k] * nq * 4096);
-    w[k].Linv = cv.take<double>(n[k] * bb);
+    w[k].tinv = V ? nullptr : cv.take<double>(n[k] * nq * 4096);
+    w[k].Linv = V ? const_cast<double*>(V[k]) : cv.take<double>(n[k] * bb);
     w[k].G = cv.take<double>(bb);
     w[k].S = cv.take<double>(bb);
     w[k].Ga = cv.take<double>(ab + 1);
@@ -472,8 +482,10 @@ int bta_pobtasi_batched_ex(bta_handle_t h, int count, const int64_t* n, const in
   }
   std::vector<GemmProb> ptip;
   for (int k = 0; k < count; ++k) {
-    if (diag_tile_inverses(D[k], (int)n[k], (int)b[k], w[k].tinv, s)) return BTA_ERR_CUDA;
-    if (block_trtri(D[k], w[k].tinv, 0, (int)n[k], (int)b[k], w[k].Linv, s)) return BTA_ERR_CUDA;
+    if (!V) {
+      if (diag_tile_inverses(D[k], (int)n[k], (int)b[k], w[k].tinv, s)) return BTA_ERR_CUDA;
+      if (block_trtri(D[k], w[k].tinv, 0, (int)n[k], (int)b[k], w[k].Linv, s)) return BTA_ERR_CUDA;
+    }
     if (a[k] > 0) {
       const int A_ = (int)a[k];
       if (diag_tile_inverses(T[k], 1, A_, w[k].tinv_t, s)) return BTA_ERR_CUDA;
@@ -537,6 +549,51 @@ int bta_pobtasi_batched_ex(bta_handle_t h, int count, const int64_t* n, const in
 int bta_pobtasi(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, double* L, double* Ab, double* T) {
   if (!h || n < 1 || b < 1 || a < 0 || !D || (n > 1 && !L) || (a > 0 && (!Ab || !T))) return BTA_ERR_INVALID;
   return bta_pobtasi_batched(h, 1, &n, &b, &a, &D, &L, &Ab, &T);
+}
+
+int bta_block_inverses(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const double* const* D,
+                       double* const* V) {
+  if (!h || count < 1 || !n || !b || !D || !V) return BTA_ERR_INVALID;
+  size_t need = kAlign;
+  for (int k = 0; k < count; ++k) {
+    if (n[k] < 1 || b[k] < 1 || !D[k] || !V[k]) return BTA_ERR_INVALID;
+    need = std::max(need, align_up((size_t)n[k] * ((b[k] + 63) / 64) * 4096 * 8));
+  }
+  int rc = ensure_ws(h, need);
+  if (rc) return rc;
+  double* tinv = reinterpret_cast<double*>(h->ws);
+  for (int k = 0; k < count; ++k) {
+    if (diag_tile_inverses(D[k], (int)n[k], (int)b[k], tinv, h->stream)) return BTA_ERR_CUDA;
+    if (block_trtri(D[k], tinv, 0, (int)n[k], (int)b[k], V[k], h->stream)) return BTA_ERR_CUDA;
+  }
+  return cuda_rc(cudaGetLastError());
+}
+
+int bta_pobtas_inv_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                           const double* const* L, const double* const* Ab, const double* const* T,
+                           const double* const* V, double* const* rhs, int trans) {
+  if (!h || count < 1 || !n || !b || !a || !V || !rhs || (trans != 0 && trans != 1)) return BTA_ERR_INVALID;
+  std::vector<int> ni(count), bi(count), ai(count);
+  std::vector<const double*> Lk(count), Abk(count), Tk(count);
+  size_t need = kAlign;
+  for (int k = 0; k < count; ++k) {
+    if (n[k] < 1 || b[k] < 1 || a[k] < 0 || !V[k] || !rhs[k] || (n[k] > 1 && (!L || !L[k])) ||
+        (a[k] > 0 && (!Ab || !T || !Ab[k] || !T[k])) || b[k] > INT32_MAX / 2)
+      return BTA_ERR_INVALID;
+    ni[k] = (int)n[k];
+    bi[k] = (int)b[k];
+    ai[k] = (int)a[k];
+    Lk[k] = n[k] > 1 ? L[k] : nullptr;
+    Abk[k] = a[k] > 0 ? Ab[k] : nullptr;
+    Tk[k] = a[k] > 0 ? T[k] : nullptr;
+    need += sweep_inv_work(bi[k]) * sizeof(double);
+  }
+  int rc = ensure_ws(h, align_up(need));
+  if (rc) return rc;
+  return sweep_inv_batched(count, ni.data(), bi.data(), ai.data(), Lk.data(), Abk.data(), Tk.data(), V, rhs, trans,
+                           reinterpret_cast<double*>(h->ws), h->stream)
+             ? BTA_ERR_CUDA
+             : BTA_OK;
 }
 
 int bta_gemm(bta_handle_t h, int precision, int64_t M, int64_t N, int64_t K, double alpha, const double* A,

@@ -36,6 +36,14 @@ int sweep_launch_batched(SweepBatch& B, cudaStream_t s);
 int arrow_forward(const double* Ab, const double* T, double* x, int n, int b, int a, cudaStream_t s);
 int arrow_backward(const double* T, double* x, int n, int b, int a, cudaStream_t s);
 
+// Sweeps with precomputed block inverses V (solve_inv.cu): count instances,
+// x[k] of length n[k] b[k] + a[k]; work holds sweep_inv_work(b[k]) doubles
+// per instance.
+size_t sweep_inv_work(int b);
+int sweep_inv_batched(int count, const int* n, const int* b, const int* a, const double* const* L,
+                      const double* const* Ab, const double* const* T, const double* const* V, double* const* x,
+                      int trans, double* work, cudaStream_t s);
+
 // Full inverses of the lower-triangular factor blocks D[i0..i1) -> out
 // (i1-i0 blocks of b x b, zeros above the diagonal); tile_inv holds the
 // inverses of their diagonal tiles (from diag_tile_inverses, same indexing).

@@ -167,6 +167,8 @@ class _Slot:
         self.gvec = torch.zeros(nobs, **f64)  # y - e exp(eta)
         self.hvec = torch.zeros(nobs, **f64)
         self.Sc = None  # copy of Q_c's factor, selected-inverted (allocated on first use)
+        self.Vc = None  # inverses of the diagonal factor blocks of Q_c / Q_prior (allocated on first use)
+        self.Vp = None
         # one pinned host buffer per assembly so that queued copies never race
         self.coef_host = [torch.zeros(nb4, dtype=torch.float64).pin_memory() for _ in range(2)]
         self.coef_dev = [torch.zeros(nb4, **f64) for _ in range(2)]
@@ -453,11 +455,35 @@ class SpatioTemporalModel:
         self._check(self.lib.bta_pobtaf_batched(self.h.bind_stream(), k, n, b, a, D, L, Ab, T, None),
                     "pobtaf_batched")
 
-    def selinv_batched(self, mats, precision="fp64"):
+    def selinv_batched(self, mats, precision="fp64", Vs=None):
         self.work["selinv_gemm"] += sum(selinv_gemm_flops(m.n, m.b, m.a) for m in mats)
         k, n, b, a, D, L, Ab, T = self._batched_args(mats)
-        self._check(self.lib.bta_pobtasi_batched_ex(self.h.bind_stream(), k, n, b, a, D, L, Ab, T,
-                                                    _PRECISIONS[precision]), "pobtasi_batched")
+        V = None if Vs is None else (ctypes.c_void_p * k)(*[v.data_ptr() for v in Vs])
+        self._check(self.lib.bta_pobtasi_batched_v(self.h.bind_stream(), k, n, b, a, D, L, Ab, T, V,
+                                                   _PRECISIONS[precision]), "pobtasi_batched")
+
+    def block_inverses(self, mats, Vs):
+        """V = inverses of the diagonal factor blocks of every matrix."""
+        k, n, b, a, D, L, Ab, T = self._batched_args(mats)
+        V = (ctypes.c_void_p * k)(*[v.data_ptr() for v in Vs])
+        self._check(self.lib.bta_block_inverses(self.h.bind_stream(), k, n, b, D, V), "block_inverses")
+
+    def sweep_inv_batched(self, mats, Vs, xs, trans):
+        """Triangular sweeps through the block inverses (n dependent steps)."""
+        k, n, b, a, D, L, Ab, T = self._batched_args(mats)
+        V = (ctypes.c_void_p * k)(*[v.data_ptr() for v in Vs])
+        X = (ctypes.c_void_p * k)(*[x.data_ptr() for x in xs])
+        self._check(self.lib.bta_pobtas_inv_batched(self.h.bind_stream(), k, n, b, a, L, Ab, T, V, X, trans),
+                    "pobtas_inv_batched")
+
+    def _slot_inverses(self, sl):
+        import torch
+
+        if sl.Vc is None:
+            nbb = self.nt * self.b * self.b
+            sl.Vc = torch.empty(nbb, dtype=torch.float64, device=self.device)
+            sl.Vp = torch.empty(nbb, dtype=torch.float64, device=self.device)
+        return sl.Vc, sl.Vp
 
     def logdet_to(self, M: BTAMatrix, out):
         D, _, _, T = M.ptrs()
@@ -705,15 +731,20 @@ class SpatioTemporalModel:
             self._gauss_conditional(th, sl)
             self.assemble_prior_bt(th, sl)
         self.factor_batched([sl.Qc for sl in sls] + [sl.Qp for sl in sls])
+        # inverses of the diagonal factor blocks: the sweeps become n dependent
+        # matrix-vector steps, and the selected inversions reuse them
+        Vc = [self._slot_inverses(sl)[0] for sl in sls]
+        Vp = [self._slot_inverses(sl)[1] for sl in sls]
+        self.block_inverses([sl.Qc for sl in sls] + [sl.Qp for sl in sls], Vc + Vp)
         for sl, th in zip(sls, thetas):
             self.logdet_to(sl.Qc, sl.scal[0:1])
             self.logdet_to(sl.Qp, sl.scal[2:3])
             self._gauss_rhs(th, sl)
             sl.x.copy_(sl.rhs)
-        self.sweep_batched([sl.Qc for sl in sls], [sl.x for sl in sls], 0)
+        self.sweep_inv_batched([sl.Qc for sl in sls], Vc, [sl.x for sl in sls], 0)
         for sl in sls:
             self.dot_to(sl.x, sl.x, sl.scal[1:2])  # b^T Q^-1 b = |L^-1 b|^2
-        self.sweep_batched([sl.Qc for sl in sls], [sl.x for sl in sls], 1)  # mu
+        self.sweep_inv_batched([sl.Qc for sl in sls], Vc, [sl.x for sl in sls], 1)  # mu
         for sl in sls:
             # per variate |A_v mu|^2 and (A_v mu)^T y_v; mu^T (E_tt' (x) K) mu per sub-block
             self.spmv(self.A_rowptr, self.A_col, self.A_val, self.nobs, sl.x, sl.eta)
@@ -723,7 +754,7 @@ class SpatioTemporalModel:
             self._check(self.lib.bta_block_quad_mv(stream, n, ns, nv, *pat, _lib.ptr(sl.x), _lib.ptr(sl.quad_st)),
                         "block_quad")
         # selected inverses and their contractions
-        self.selinv_batched([sl.Qc for sl in sls] + [sl.Qp for sl in sls], precision)
+        self.selinv_batched([sl.Qc for sl in sls] + [sl.Qp for sl in sls], precision, Vc + Vp)
         for sl in sls:
             Dc, Lc, _, _ = sl.Qc.ptrs()
             Dp, Lp, _, _ = sl.Qp.ptrs()

@@ -98,6 +98,26 @@ int bta_pobtasi_batched_ex(bta_handle_t h, int count, const int64_t* n, const in
                            int precision);
 
 /*
+ * Inverses of the diagonal factor blocks, V[k][i] = L_ii^-1 (n[k] blocks of
+ * b[k] x b[k], lower triangular, zeros above the diagonal) into caller
+ * buffers; with them a triangular sweep is n dependent steps of two
+ * bandwidth-bound matrix-vector products (bta_pobtas_inv_batched: same
+ * trans and rhs conventions as bta_pobtas_batched; D is not read), and the
+ * selected inversion skips its own block inversion
+ * (bta_pobtasi_batched_v; V == NULL computes them as bta_pobtasi_batched_ex
+ * does).  No counterpart in the reference: Serinv's pobtas solves with the
+ * factor blocks directly.
+ */
+int bta_block_inverses(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const double* const* D,
+                       double* const* V);
+int bta_pobtas_inv_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                           const double* const* L, const double* const* Ab, const double* const* T,
+                           const double* const* V, double* const* rhs, int trans);
+int bta_pobtasi_batched_v(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                          double* const* D, double* const* L, double* const* Ab, double* const* T,
+                          const double* const* V, int precision);
+
+/*
  * C = beta C + alpha op(A) op(B) (row-major FP64; op(A)[m][k] = A[m*lda+k], or
  * A[k*lda+m] with a_trans; op(B)[k][n] = B[n*ldb+k], or B[k*ldb+n] with b_kn)
  * with the library's grouped GEMM in the given BTA_PREC_* arithmetic, on the

@@ -161,3 +161,47 @@ def test_batched_factor_and_selinv_match_single():
             if x.numel():
                 assert rel(y.cpu().numpy(), x.cpu().numpy()) < TOL
                 assert rel(y.cpu().numpy(), S[j]) < TOL
+
+
+@pytest.mark.parametrize("n,b,a", SHAPES)
+def test_block_inverse_sweeps_and_selinv(n, b, a):
+    """bta_block_inverses + bta_pobtas_inv_batched (two sweeps) against a dense
+    solve, and bta_pobtasi_batched_v with those inverses against the oracle."""
+    import ctypes
+
+    import torch
+
+    from dalia_b200 import _lib
+
+    lib = _lib.load()
+    h = _lib.handle()
+    rng = np.random.default_rng(11 * n + b + a)
+    D, L, Ab, T = bta_ref.random_bta(n, b, a, rng)
+    M = bta_ref.bta_to_dense(D, L, Ab, T)
+    d = _cuda(D, L, Ab, T)
+    V = torch.empty(n * b * b, dtype=torch.float64, device="cuda")
+    arr = lambda t: (ctypes.c_void_p * 1)(t.data_ptr() if (t is not None and t.numel()) else None)
+    i64 = lambda v: (ctypes.c_int64 * 1)(v)
+    sz = (i64(n), i64(b), i64(a))
+    _lib.check(lib.bta_pobtaf_batched(h.bind_stream(), 1, *sz, arr(d[0]), arr(d[1]), arr(d[2]), arr(d[3]), None),
+               "pobtaf")
+    _lib.check(lib.bta_block_inverses(h.bind_stream(), 1, sz[0], sz[1], arr(d[0]), arr(V)), "inverses")
+    rhs = rng.standard_normal(n * b + a)
+    x = _cuda(rhs)[0]
+    for trans in (0, 1):
+        _lib.check(lib.bta_pobtas_inv_batched(h.bind_stream(), 1, *sz, arr(d[1]), arr(d[2]), arr(d[3]), arr(V),
+                                              arr(x), trans), "sweep")
+    st = ctypes.c_int64(0)
+    _lib.check(lib.bta_get_status(h.bind_stream(), ctypes.byref(st)), "status")
+    assert rel(x.cpu().numpy(), np.linalg.solve(M, rhs)) < TOL
+    ref = [v.copy() for v in (D, L, Ab, T)]
+    bta_ref.pobtaf(*ref)
+    bta_ref.pobtasi(*ref)
+    _lib.check(lib.bta_pobtasi_batched_v(h.bind_stream(), 1, *sz, arr(d[0]), arr(d[1]), arr(d[2]), arr(d[3]), arr(V),
+                                         _lib.BTA_PREC_FP64), "pobtasi_v")
+    got = _np(*d)
+    assert rel(got[0], ref[0]) < TOL
+    if n > 1:
+        assert rel(got[1], ref[1]) < TOL
+    if a:
+        assert rel(got[2], ref[2]) < TOL and rel(got[3], ref[3]) < TOL
