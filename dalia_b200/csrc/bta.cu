@@ -113,7 +113,8 @@ int get_tasks(bta_context* h, const std::vector<PanelInst>& insts, const int4** 
   for (const auto& I : insts) {
     key.push_back(I.b);
     key.push_back(I.a);
-    key.push_back((I.L != nullptr ? 1 : 0) | (I.Ttip != nullptr ? 2 : 0));
+    key.push_back((I.L != nullptr ? 1 : 0) | (I.Ttip != nullptr ? 2 : 0) | (I.Lprev != nullptr ? 4 : 0) |
+                  (I.Abprev != nullptr ? 8 : 0));
   }
   auto it = h->tasks.find(key);
   if (it == h->tasks.end()) {
@@ -159,7 +160,7 @@ int run_panels(bta_context* h, const std::vector<PanelSpec>& specs, Carve& cv) {
       I.Abprev = aa ? sp.Abprev : nullptr;
       I.Ttip = (aa > 0 && aa <= 64) ? sp.Ttip : nullptr;
       I.Linv = cv.take<double>((size_t)I.nq * 64 * 64);
-      cnt_total += (size_t)2 * I.nrows_t * I.nq;
+      cnt_total += (size_t)3 * I.nrows_t * I.nq;
       insts.push_back(I);
     }
     int* cnt = cv.take<int>(cnt_total + 4);
@@ -167,7 +168,8 @@ int run_panels(bta_context* h, const std::vector<PanelSpec>& specs, Carve& cv) {
     for (auto& I : insts) {
       I.upd = cnt + off;
       I.flag = cnt + off + (size_t)I.nrows_t * I.nq;
-      off += (size_t)2 * I.nrows_t * I.nq;
+      I.prv = cnt + off + (size_t)2 * I.nrows_t * I.nq;
+      off += (size_t)3 * I.nrows_t * I.nq;
     }
     const int4* tasks;
     int ntasks;
@@ -189,7 +191,7 @@ int run_panels(bta_context* h, const std::vector<PanelSpec>& specs, Carve& cv) {
 size_t panel_ws_bytes(int b, int a) {
   const int nq = (b + 63) / 64;
   const int nr = panel_rows(b, a, true);
-  return align_up((size_t)nq * 4096 * 8) + align_up(((size_t)2 * nr * nq + 4) * 4) + 2 * kAlign;
+  return align_up((size_t)nq * 4096 * 8) + align_up(((size_t)3 * nr * nq + 4) * 4) + 2 * kAlign;
 }
 
 int reset_status(bta_context* h) {

@@ -94,18 +94,24 @@ __device__ __forceinline__ TileRef prev_tile_of(const PanelInst& I, int p, int c
   } else if (I.L != nullptr && p < 2 * I.nq) {
     t.ptr = nullptr;
     t.rows = 0;
-  } else {
+  } else if (I.Abprev != nullptr) {
     const int ar = p - I.nq - (I.L != nullptr ? I.nq : 0);
     t.ptr = const_cast<double*>(I.Abprev) + (size_t)(ar * T) * I.b + c * T;
     t.rows = min(T, I.a - ar * T);
+  } else {
+    t.ptr = nullptr;
+    t.rows = 0;
   }
   return t;
 }
 
-// The previous block column's Schur update streams whole 64-row blocks of
-// Lprev / Abprev through a ring of 16-wide k-slabs, so loading slab s+2
-// overlaps the DMMA work on slab s (it needs no dependency waits: that column
-// is final before the launch).
+// Whether tile (p, r) receives a previous-column term (its own TASK_PREV).
+__device__ __forceinline__ bool has_prev(const PanelInst& I, int p) {
+  return I.Lprev != nullptr && prev_tile_of(I, p, 0).rows > 0;
+}
+
+// Accumulations stream whole 64-row strips through a ring of 16-wide k-slabs,
+// so loading slab s+2 overlaps the DMMA work on slab s.
 constexpr int PK = 16;
 constexpr int PSK = PK + 4;  // slab row stride: conflict-light DMMA fragment loads
 constexpr int PST = 3;
@@ -113,7 +119,8 @@ constexpr int PSLAB = T * PSK;
 static_assert(2 * PST * PSLAB <= 2 * T * SG, "slab ring exceeds the two tile buffers");
 
 // 64 x 16 slab of a row block at g (row stride ld): rows < rows and columns
-// k0 .. k0+15 < kmax, zero-filled elsewhere.
+// k0 .. k0+15 < kmax, zero-filled elsewhere.  Reads bypass L1: the strips of
+// this panel are written by other CTAs during the launch.
 __device__ __forceinline__ void load_slab(double* s, const double* g, int ld, int rows, int k0, int kmax, bool vec,
                                           int tid) {
 #pragma unroll
@@ -125,11 +132,16 @@ __device__ __forceinline__ void load_slab(double* s, const double* g, int ld, in
     const bool v0 = r < rows && gk < kmax;
     const bool v1 = r < rows && gk + 1 < kmax;
     const double* src = g + (size_t)r * ld + gk;
-    if (vec && v1) {
-      cp_async16(d, src, true);
+    if (vec) {
+      if (v1) {
+        cp_async16(d, src, true);
+      } else {
+        d[0] = v0 ? __ldcg(src) : 0.0;
+        d[1] = 0.0;
+      }
     } else {
-      cp_async8(d, v0 ? src : g, v0);
-      cp_async8(d + 1, v1 ? src + 1 : g, v1);
+      d[0] = v0 ? __ldcg(src) : 0.0;
+      d[1] = v1 ? __ldcg(src + 1) : 0.0;
     }
   }
 }
@@ -154,57 +166,57 @@ __device__ __forceinline__ void mma_slab(const double* X, const double* Y, doubl
   }
 }
 
-// acc += Xrow(p) Xrow(r)^T over the full width of the previous block column.
-__device__ void acc_prev_stream(const PanelInst& I, int p, int r, double* smem, double (&acc)[2][4][4], int tid,
-                                int wm, int wn, int g, int t) {
-  const TileRef x0 = prev_tile_of(I, p, 0), y0 = prev_tile_of(I, r, 0);
-  const int ld = I.b, kmax = I.b;
-  const int nslab = (kmax + PK - 1) / PK;
-  const bool vec = ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(x0.ptr) & 15) == 0) &&
-                   ((reinterpret_cast<uintptr_t>(y0.ptr) & 15) == 0);
-  double* As = smem;
-  double* Bs = smem + PST * PSLAB;
-  __syncthreads();  // the tile buffers may still be read by the previous step
-#pragma unroll
-  for (int st = 0; st < PST - 1; ++st) {
-    if (st < nslab) {
-      load_slab(As + st * PSLAB, x0.ptr, ld, x0.rows, st * PK, kmax, vec, tid);
-      load_slab(Bs + st * PSLAB, y0.ptr, ld, y0.rows, st * PK, kmax, vec, tid);
-    }
-    cp_async_commit();
-  }
-  for (int s = 0; s < nslab; ++s) {
-    cp_async_wait<PST - 2>();
-    __syncthreads();
-    const int nx = s + PST - 1;
-    if (nx < nslab) {
-      load_slab(As + (nx % PST) * PSLAB, x0.ptr, ld, x0.rows, nx * PK, kmax, vec, tid);
-      load_slab(Bs + (nx % PST) * PSLAB, y0.ptr, ld, y0.rows, nx * PK, kmax, vec, tid);
-    }
-    cp_async_commit();
-    mma_slab(As + (s % PST) * PSLAB, Bs + (s % PST) * PSLAB, acc, wm, wn, g, t);
-  }
-  cp_async_wait<0>();
-  __syncthreads();
-}
-
-// acc += X Y^T for two global tiles (staged through the two smem buffers).
-__device__ __forceinline__ void acc_pair(const TileRef& x, const TileRef& y, double* bufA, double* bufL, int ld,
-                                         double (&acc)[2][4][4], int tid, int wm, int wn, int g, int t) {
-  load_async<SG>(bufA, x.ptr, ld, x.rows, x.cols, tid);
-  load_async<SG>(bufL, y.ptr, ld, y.rows, y.cols, tid);
-  cp_async_commit();
-  cp_async_wait<0>();
-  __syncthreads();
-  mma_nt(bufA, bufL, (x.cols + 3) & ~3, acc, wm, wn, g, t);
-  __syncthreads();
-}
-
 // Block-wide wait by thread 0; returns the verdict to every thread.
 __device__ __forceinline__ bool block_wait(const int* p, int target, int* abort_flag, int* s_ok) {
   if (threadIdx.x == 0) *s_ok = wait_ge(p, target, abort_flag) ? 1 : 0;
   __syncthreads();
   return *s_ok != 0;
+}
+
+// acc += X Y^T over columns [0, kcols) of two 64-row strips x (xrows valid
+// rows) and y (yrows valid rows), row stride ld.  With gates, the columns of
+// tile k are loaded only once gx[k] and gy[k] are set (their producers
+// finished).  Returns false when such a wait gave up.
+__device__ bool acc_stream(const double* x, int xrows, const double* y, int yrows, int ld, int kcols, const int* gx,
+                           const int* gy, int* abort_flag, int* s_ok, double* smem, double (&acc)[2][4][4], int tid,
+                           int wm, int wn, int g, int t) {
+  const int nslab = (kcols + PK - 1) / PK;
+  if (nslab == 0) return true;
+  const bool vec = ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0) &&
+                   ((reinterpret_cast<uintptr_t>(y) & 15) == 0);
+  double* As = smem;
+  double* Bs = smem + PST * PSLAB;
+  bool ok = true;
+  // issue slab j (after its gate, at the first slab of every tile)
+  auto issue = [&](int j) {
+    if (gx != nullptr && ok && (j * PK) % T == 0) {
+      const int k = (j * PK) / T;
+      if (tid == 0) *s_ok = (wait_ge(gx + k, 1, abort_flag) && wait_ge(gy + k, 1, abort_flag)) ? 1 : 0;
+      __syncthreads();
+      ok = *s_ok != 0;
+    }
+    if (ok) {
+      load_slab(As + (j % PST) * PSLAB, x, ld, xrows, j * PK, kcols, vec, tid);
+      load_slab(Bs + (j % PST) * PSLAB, y, ld, yrows, j * PK, kcols, vec, tid);
+    }
+  };
+  __syncthreads();  // the tile buffers may still be read by the previous step
+#pragma unroll
+  for (int st = 0; st < PST - 1; ++st) {
+    if (st < nslab) issue(st);
+    cp_async_commit();
+  }
+  for (int s = 0; s < nslab && ok; ++s) {
+    cp_async_wait<PST - 2>();
+    __syncthreads();
+    const int nx = s + PST - 1;
+    if (nx < nslab) issue(nx);
+    cp_async_commit();
+    if (ok) mma_slab(As + (s % PST) * PSLAB, Bs + (s % PST) * PSLAB, acc, wm, wn, g, t);
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  return ok;
 }
 
 __device__ __forceinline__ void release(int* p, int v) {
@@ -306,6 +318,28 @@ __device__ void run_chain(const PanelInst& I, double* bufA, double* bufL, double
   }
 }
 
+// Writes tile -= acc over its valid rows x cols (L2 reads: other CTAs wrote it).
+__device__ __forceinline__ void sub_acc(const TileRef& c, int ld, const double (&acc)[2][4][4], int wm, int wn, int g,
+                                        int t) {
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int row = wm * 32 + mi * 16 + g + h * 8;
+      if (row >= c.rows) continue;
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int col = wn * 32 + ni * 8 + 2 * t + e;
+          if (col < c.cols) {
+            double* dst = c.ptr + (size_t)row * ld + col;
+            *dst = __ldcg(dst) - acc[mi][ni][h * 2 + e];
+          }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant__ PanelBatch B) {
   extern __shared__ __align__(16) double sm[];
   double* bufA = sm;
@@ -334,25 +368,27 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
     const int kind = tk.y, p = tk.z, r = tk.w;
     const int nq = I.nq, ld = I.b;
     TRACE_T0();
-    // left-looking accumulation of tile(p, r) -= sum_k X(p, k) X(r, k)^T:
-    // first the previous block column's terms (final before this launch),
-    // then this panel's columns as they become final
     double acc[2][4][4];
     zero_acc(acc);
+    if (kind == TASK_PREV) {
+      // tile(p, r) -= Xprev(p) Xprev(r)^T: that column is final before the launch
+      const TileRef xp = prev_tile_of(I, p, 0), yp = prev_tile_of(I, r, 0);
+      acc_stream(xp.ptr, xp.rows, yp.ptr, yp.rows, ld, I.b, nullptr, nullptr, B.abort_flag, &s_ok, bufA, acc, tid,
+                 wm, wn, g, t);
+      TRACE_T1();
+      sub_acc(tile_of(I, p, r), ld, acc, wm, wn, g, t);
+      release(&I.prv[p * nq + r], 1);
+      TRACE(kind, p, r);
+      continue;
+    }
     if (kind == TASK_TIP) {
-      // T -= sum_k X(arrow, k) X(arrow, k)^T once the arrow row is final
+      // T -= sum_k X(arrow, k) X(arrow, k)^T as the arrow row becomes final
       const int pa = I.nrows_t - 1;
-      bool okt = true;
-      for (int k = 0; k < nq && okt; ++k) {
-        if (tid == 0) s_ok = wait_ge(&I.flag[pa * nq + k], 1, B.abort_flag) ? 1 : 0;
-        __syncthreads();
-        okt = s_ok != 0;
-        if (okt) {
-          const TileRef xa = tile_of(I, pa, k);
-          acc_pair(xa, xa, bufA, bufL, ld, acc, tid, wm, wn, g, t);
-        }
-      }
-      if (!okt) continue;
+      const TileRef xa = tile_of(I, pa, 0);
+      const int* gate = I.flag + pa * nq;
+      if (!acc_stream(xa.ptr, xa.rows, xa.ptr, xa.rows, ld, I.b, gate, gate, B.abort_flag, &s_ok, bufA, acc, tid,
+                      wm, wn, g, t))
+        continue;
 #pragma unroll
       for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -369,10 +405,6 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
         }
       continue;
     }
-    if (I.Lprev != nullptr) {
-      const TileRef yp0 = prev_tile_of(I, r, 0);
-      if (prev_tile_of(I, p, 0).rows > 0 && yp0.rows > 0) acc_prev_stream(I, p, r, bufA, acc, tid, wm, wn, g, t);
-    }
     // zero the mirrored strictly-upper tile (r, p) of the diagonal block
     if (p < nq && p > r) {
       double* up = I.D + (size_t)(r * T) * ld + p * T;
@@ -382,39 +414,22 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
         if (k < cw) up[(size_t)i * ld + k] = 0.0;
       }
     }
+    // left-looking accumulation of tile(p, r) -= sum_{k < kmax} X(p, k) X(r, k)^T
+    // as the source columns become final
     const int kmax = (kind == TASK_AGG_DIAG) ? r - 1 : r;
-    bool ok = true;
-    for (int k = 0; k < kmax && ok; ++k) {
-      if (tid == 0)
-        s_ok = (wait_ge(&I.flag[p * nq + k], 1, B.abort_flag) && wait_ge(&I.flag[r * nq + k], 1, B.abort_flag)) ? 1
-                                                                                                                : 0;
-      __syncthreads();
-      ok = s_ok != 0;
-      if (!ok) break;
-      acc_pair(tile_of(I, p, k), tile_of(I, r, k), bufA, bufL, ld, acc, tid, wm, wn, g, t);
+    {
+      const TileRef xs = tile_of(I, p, 0), ys = tile_of(I, r, 0);
+      if (!acc_stream(xs.ptr, xs.rows, ys.ptr, ys.rows, ld, max(kmax, 0) * T, I.flag + p * nq, I.flag + r * nq,
+                      B.abort_flag, &s_ok, bufA, acc, tid, wm, wn, g, t))
+        continue;
     }
-    if (!ok) continue;
+    // the previous column's term of this tile has been applied
+    if (has_prev(I, p) && !block_wait(&I.prv[p * nq + r], 1, B.abort_flag, &s_ok)) continue;
     TRACE_T1();
     const TileRef c = tile_of(I, p, r);
     if (kind != TASK_AGG_TRSM) {
       // chain input: write the accumulated tile, the chain CTA finishes it
-#pragma unroll
-      for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int row = wm * 32 + mi * 16 + g + h * 8;
-          if (row >= c.rows) continue;
-#pragma unroll
-          for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-              const int col = wn * 32 + ni * 8 + 2 * t + e;
-              if (col < c.cols) {
-                double* dst = c.ptr + (size_t)row * ld + col;
-                *dst = __ldcg(dst) - acc[mi][ni][h * 2 + e];
-              }
-            }
-        }
+      sub_acc(c, ld, acc, wm, wn, g, t);
       release(&I.upd[p * nq + r], 1);
       TRACE(kind, p, r);
       continue;
@@ -476,19 +491,50 @@ extern "C" int bta_trace_setup(unsigned long long* buf) {
 // Queue order: one task per tile, column by column; within a column the two
 // tiles the chain CTA consumes next (the diagonal tile and the one below it)
 // come first, then the remaining rows of the diagonal block, then the rows of
-// the block below and of the arrow.  Every task only waits on outputs of
-// earlier columns or of the chain, so the order is topological.  Instances
-// are interleaved column by column.
+// the block below and of the arrow.  Every such task only waits on outputs of
+// earlier columns or of the chain, so the order is topological.  The
+// previous-column tasks wait on nothing; those of column r + PREV_LOOKAHEAD
+// are queued before column r's tasks (diagonal and sub-diagonal tiles first),
+// so the term is applied before the chain needs the tile.  Instances are
+// interleaved column by column.
+namespace {
+
+bool host_has_prev(const PanelInst& I, int p) {
+  if (I.Lprev == nullptr) return false;
+  if (p < I.nq) return true;
+  if (I.L != nullptr && p < 2 * I.nq) return false;
+  return I.Abprev != nullptr;
+}
+
+void prev_tasks(const std::vector<PanelInst>& insts, int c, std::vector<int4>& tasks) {
+  for (int ii = 0; ii < (int)insts.size(); ++ii) {
+    const PanelInst& I = insts[ii];
+    if (c >= I.nq || I.Lprev == nullptr) continue;
+    for (int p = c; p < std::min(c + 2, I.nq); ++p) tasks.push_back(make_int4(ii, TASK_PREV, p, c));
+  }
+  for (int ii = 0; ii < (int)insts.size(); ++ii) {
+    const PanelInst& I = insts[ii];
+    if (c >= I.nq || I.Lprev == nullptr) continue;
+    for (int p = std::min(c + 2, I.nq); p < I.nrows_t; ++p)
+      if (host_has_prev(I, p)) tasks.push_back(make_int4(ii, TASK_PREV, p, c));
+  }
+}
+
+}  // namespace
+
 void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks) {
   int max_nq = 0;
   for (const auto& I : insts) max_nq = std::max(max_nq, I.nq);
+  int prev_done = -1;  // last column whose previous-column tasks are queued
   for (int r = 0; r < max_nq; ++r) {
+    if (prev_done < r) prev_tasks(insts, ++prev_done, tasks);
     for (int ii = 0; ii < (int)insts.size(); ++ii) {
       const PanelInst& I = insts[ii];
       if (r >= I.nq) continue;
       tasks.push_back(make_int4(ii, TASK_AGG_DIAG, r, r));
       if (r + 1 < I.nq) tasks.push_back(make_int4(ii, TASK_AGG_SUB, r + 1, r));
     }
+    while (prev_done < std::min(r + PREV_LOOKAHEAD, max_nq - 1)) prev_tasks(insts, ++prev_done, tasks);
     for (int ii = 0; ii < (int)insts.size(); ++ii) {
       const PanelInst& I = insts[ii];
       if (r >= I.nq) continue;

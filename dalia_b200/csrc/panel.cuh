@@ -5,16 +5,17 @@
 // tiles with nq = ceil(b/64) tile columns, and factored in place:
 //   X(p, r) = (A(p, r) - sum_{k<r} X(p, k) X(r, k)^T) Linv_r^T   (p > r)
 //   L_rr    = chol(A(r, r) - sum_{k<r} X(r, k) X(r, k)^T),  Linv_r = L_rr^-1
-// When Lprev / Abprev are given, every tile task first applies the previous
-// block column's Schur update (D -= Lprev Lprev^T, Ab -= Abprev Lprev^T) and
+// When Lprev / Abprev are given, the previous block column's Schur update
+// (D -= Lprev Lprev^T, Ab -= Abprev Lprev^T) is applied by one dependency-free
+// task per tile, queued a few tile columns ahead of the tile's own task, and
 // a tip task applies T -= Ab Ab^T, so a whole BTA step is one launch.
 // The critical path -- X(q, q-1), the last update of tile (q, q), POTRF(q) and
 // Linv_q for q = 0..nq-1 -- runs in one dedicated "chain" CTA per instance that
 // keeps Linv_{q-1} in shared memory.  Every other tile is one left-looking task
 // claimed from a queue in a fixed topological order by the remaining
-// persistent CTAs: it accumulates its updates in registers as the source
-// columns become final, then applies its TRSM (or hands the tile to the
-// chain).  Dependencies are release/acquire flags per tile; every wait is
+// persistent CTAs: it streams its row strips through a shared-memory ring,
+// accumulating in registers as the source columns become final, then applies
+// its TRSM (or hands the tile to the chain).  Dependencies are release/acquire flags per tile; every wait is
 // bounded and sets an abort flag instead of hanging.
 #pragma once
 
@@ -35,6 +36,7 @@ struct PanelInst {
   double* Ttip;          // arrow tip (a x a, a <= 64) updated by this panel, or nullptr
   int* upd;      // [nrows_t * nq] chain input tile accumulated (set to 1)
   int* flag;     // [nrows_t * nq] tile final (X computed; diagonal: Linv ready)
+  int* prv;      // [nrows_t * nq] previous column's update applied (when Lprev)
   unsigned long long* info;  // min failing pivot (1-based global index)
   long long pivot_base;      // global row index of D's first row
   int b, a, nq, nrows_t;
@@ -56,7 +58,12 @@ struct PanelBatch {
 // the diagonal), or accumulation followed by the TRSM with the inverse of the
 // column's diagonal tile.
 // TASK_TIP subtracts the panel's arrow rows from the tip: T -= X_a X_a^T.
-enum : int { TASK_AGG_DIAG = 3, TASK_AGG_SUB = 4, TASK_AGG_TRSM = 5, TASK_TIP = 6 };
+// TASK_PREV applies the previous block column's term to one tile (no waits).
+enum : int { TASK_AGG_DIAG = 3, TASK_AGG_SUB = 4, TASK_AGG_TRSM = 5, TASK_TIP = 6, TASK_PREV = 7 };
+
+// Tile columns by which the previous-column tasks run ahead of the tiles'
+// own tasks in the queue.
+constexpr int PREV_LOOKAHEAD = 2;
 
 // Number of tile rows of a panel (diag rows, lower rows, arrow rows).
 inline int panel_rows(int b, int a, bool has_L) {
