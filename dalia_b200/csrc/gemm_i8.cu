@@ -19,8 +19,10 @@
 // slice_kernel (digits, written as the 32-byte-swizzled K-major shared-memory
 // images the MMA reads), gemm_i8_kernel: one producer thread bulk-copies the
 // digit images of a 32-wide k-slab (A: 128 rows x OZ_S digits, B: 64 rows x
-// OZ_S digits, no multicast) into a 4-stage ring; one thread issues the 28
-// (p, q) MMAs of the slab, each into the TMEM accumulator of d = p + q; four
+// OZ_S digits, no multicast) into a 4-stage ring; one thread issues the
+// products of the slab, one MMA per A digit p against the stacked B digits
+// (N up to 256: 10 MMAs for 28 digit pairs), each pair (p, q) landing in the
+// TMEM accumulator of d = p + q; four
 // epilogue warps read the OZ_S accumulators (tcgen05.ld), rescale and write C
 // in FP64.  Every wait is bounded and raises the abort flag on timeout.
 #include <algorithm>
@@ -50,8 +52,10 @@ static_assert(OZ_S * QBN <= TMEM_COLS, "accumulators exceed tensor memory");
 
 // Instruction descriptor: D S32 (bits 4-5 = 2), A and B signed 8-bit (bits
 // 7-9, 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
-constexpr uint32_t IDESC_I8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(QBN >> 3) << 17) |
-                              ((uint32_t)(QBM >> 4) << 24);
+__host__ __device__ constexpr uint32_t idesc_i8(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(QBM >> 4) << 24);
+}
+constexpr int QMMA_NMAX = 256;  // largest N of one M = 128 MMA
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -107,12 +111,13 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
                "l"(src), "r"(bytes), "r"(bar)
                : "memory");
 }
-__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accum) {
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accum) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(IDESC_I8), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
       : "memory");
 }
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&v)[32]) {
@@ -383,14 +388,20 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
         tc_fence_after();
         const uint32_t a0 = stage0 + st * QSTAGE_BYTES, b0 = a0 + OZ_S * A_SLICE;
 #pragma unroll
-        for (int p = 0; p < OZ_S; ++p)
+        for (int p = 0; p < OZ_S; ++p) {
+          // digit p of A against the stacked digit images q = q0 .. q0+nq-1 of
+          // B (consecutive 64-row images form one K-major operand of 64 nq
+          // rows): product (p, q) lands in columns (p + q) QBN .. of tensor
+          // memory, the accumulator of d = p + q.  The first products of the
+          // tile, p = 0 at step 0, overwrite every accumulator.
+          const uint32_t acc = (step > 0 || p > 0) ? 1u : 0u;
 #pragma unroll
-          for (int q = 0; q + p < OZ_S; ++q) {
-            // digits p, q (0-based): accumulator d = p + q; its first product
-            // of the tile, (p, q) = (0, d) at step 0, overwrites it
-            const uint32_t acc = (step > 0 || p > 0) ? 1u : 0u;
-            mma_i8(tmem + (uint32_t)((p + q) * QBN), sw32_desc(a0 + p * A_SLICE), sw32_desc(b0 + q * B_SLICE), acc);
+          for (int q0 = 0; q0 < OZ_S - p; q0 += QMMA_NMAX / QBN) {
+            const int nq = min(QMMA_NMAX / QBN, OZ_S - p - q0);
+            mma_i8(tmem + (uint32_t)((p + q0) * QBN), sw32_desc(a0 + p * A_SLICE), sw32_desc(b0 + q0 * B_SLICE),
+                   idesc_i8(nq * QBN), acc);
           }
+        }
         tc_commit(empty0 + 8 * st);
       }
       tc_commit(done_bar);
