@@ -15,9 +15,9 @@
 // amplifies the truncation: five digits left gradient errors of 2e-3 at
 // b = 1500.
 //
-// Pipeline: slice_exp_kernel (row / column maxima -> exponents, atomicMax),
-// slice_kernel (digits, written as the 32-byte-swizzled K-major shared-memory
-// images the MMA reads), gemm_i8_kernel: one producer thread bulk-copies the
+// Pipeline: slice_kernel (per 32 rows of a problem side: the maxima over all
+// segments -> exponents, then the digits, written as the 32-byte-swizzled
+// K-major shared-memory images the MMA reads), gemm_i8_kernel: one producer thread bulk-copies the
 // digit images of a 32-wide k-slab (A: 128 rows x OZ_S digits, B: 64 rows x
 // OZ_S digits, no multicast) into a 4-stage ring; one thread issues the
 // products of the slab, one MMA per A digit p against the stacked B digits
@@ -137,35 +137,35 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&v)[32]) {
 }
 
 // ---------------------------------------------------------------- slicing
-// One operand of one segment: rows x K, element (r, k) at P[r*ld + k]
-// (kcontig) or P[k*ld + r], scaled by alpha; digits go to
-// out[(p*KT + kt)*RB + rb] (one 2 KB image per 64 rows x 32 k), exponents to
-// exps[rows] (shared by all segments of a problem).
-struct SliceJob {
+// One side of one problem: the op(A) (or op(B)) operands of its segments,
+// which share one exponent per image row.  Segment s: element (r, k) at
+// P[r*ld + k] (kcontig) or P[k*ld + r], scaled by alpha; its digits go to
+// out[(p*KT + kt)*RB + rb] (one 2 KB image per 64 rows x 32 k).
+struct SliceSeg {
   const double* P;
-  double alpha;
-  int* exps;
   int8_t* out;
-  int ld, rows, K, kcontig, RB, KT;
-  int unit_start;   // first work unit of this job (exponent pass)
-  int chunk_start;  // first 16-byte chunk of this job (digit pass)
+  double alpha;
+  int ld, K, kcontig, KT;
 };
 
-constexpr int SLICE_MAXJ = 160;
-constexpr int EXP_KCHUNK = 256;
+struct SliceGroup {
+  int* exps;       // exponent of every image row < rows
+  int rows;        // rows with data (M or N); image rows up to 64 RB are zero
+  int RB;          // 64-row image blocks
+  int nseg;
+  int unit_start;  // first SU-row unit of this group
+  SliceSeg s[3];
+};
+
+constexpr int SLICE_MAXG = 48;
+constexpr int SLICE_THREADS = 256;
+constexpr int SU = 32;  // image rows per slicing unit
 
 struct SliceBatch {
   int count;
   int units;
-  int chunks;
-  SliceJob job[SLICE_MAXJ];
+  SliceGroup g[SLICE_MAXG];
 };
-
-__device__ __forceinline__ int find_job(const SliceBatch& B, int idx, bool units) {
-  int j = 0;
-  while (j + 1 < B.count && idx >= (units ? B.job[j + 1].unit_start : B.job[j + 1].chunk_start)) ++j;
-  return j;
-}
 
 __device__ __forceinline__ int exponent_of(double m) {
   if (!(m > 0.0)) return EXP_NONE;
@@ -174,93 +174,194 @@ __device__ __forceinline__ int exponent_of(double m) {
   return e;
 }
 
-// Work unit: (job, group of 32 rows, chunk of EXP_KCHUNK k); one warp, one
-// lane per row of the group; combined over units and segments by atomicMax.
-__global__ void __launch_bounds__(256) slice_exp_kernel(const __grid_constant__ SliceBatch B) {
-  const int lane = threadIdx.x & 31;
-  const int warps = (gridDim.x * blockDim.x) >> 5;
-  for (int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < B.units; u += warps) {
-    const SliceJob& J = B.job[find_job(B, u, true)];
-    const int local = u - J.unit_start;
-    const int nkc = max(1, (J.K + EXP_KCHUNK - 1) / EXP_KCHUNK);
-    const int g = local / nkc, kc = local - g * nkc;
-    const int r0 = g * 32, k0 = kc * EXP_KCHUNK, k1 = min(J.K, k0 + EXP_KCHUNK);
-    double mymax = 0.0;
-    if (J.kcontig) {
-      for (int rr = 0; rr < 32 && r0 + rr < J.rows; ++rr) {
-        const double* row = J.P + (size_t)(r0 + rr) * J.ld;
-        double m = 0.0;
-        for (int k = k0 + lane; k < k1; k += 32) m = fmax(m, fabs(row[k]));
+// 4 x 4 byte transpose: out[i] byte j = in[j] byte i.
+__device__ __forceinline__ void transpose4(const uint32_t (&in)[4], uint32_t (&out)[4]) {
+  const uint32_t t0 = __byte_perm(in[0], in[1], 0x5140), t1 = __byte_perm(in[0], in[1], 0x7362);
+  const uint32_t t2 = __byte_perm(in[2], in[3], 0x5140), t3 = __byte_perm(in[2], in[3], 0x7362);
+  out[0] = __byte_perm(t0, t2, 0x5410);
+  out[1] = __byte_perm(t0, t2, 0x7632);
+  out[2] = __byte_perm(t1, t3, 0x5410);
+  out[3] = __byte_perm(t1, t3, 0x7632);
+}
+
+// Digits of one 16-k chunk (image row rg, k = 16 kc ..) of segment S with
+// exponent e, written to the swizzled K-major image.  The truncated integer
+// U = |alpha x| 2^(7 OZ_S - e) < 2^49 splits into 28 + 21 bits; each half's
+// 7-bit digits are spread to bytes (digit 3 and digit 6 in byte 0), negated
+// per byte for negative entries, and four consecutive k are transposed into
+// the digit planes (byte j of a plane word = k offset j).
+static_assert(OZ_S == 7, "the digit spreading below cuts 4 + 3 digits");
+__device__ __forceinline__ void cut_chunk(const SliceSeg& S, int RB, int rg, bool rowok, int kc, int e) {
+  const int k0 = kc * 16;
+  double xs[16];
+  if (S.kcontig && rowok && k0 + 15 < S.K && ((S.ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(S.P) & 15) == 0)) {
+    const double2* src = reinterpret_cast<const double2*>(S.P + (size_t)rg * S.ld + k0);
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if (lane == rr) mymax = m;
-      }
-    } else if (r0 + lane < J.rows) {
-      for (int k = k0; k < k1; ++k) mymax = fmax(mymax, fabs(J.P[(size_t)k * J.ld + r0 + lane]));
+    for (int j = 0; j < 8; ++j) {
+      const double2 v = src[j];
+      xs[2 * j] = v.x;
+      xs[2 * j + 1] = v.y;
     }
-    if (r0 + lane < J.rows) atomicMax(&J.exps[r0 + lane], exponent_of(fabs(J.alpha) * mymax));
+  } else {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int k = k0 + j;
+      xs[j] = (rowok && k < S.K) ? S.P[S.kcontig ? (size_t)rg * S.ld + k : (size_t)k * S.ld + rg] : 0.0;
+    }
+  }
+  // |alpha| 2^(7 OZ_S - e) is exact; products with it round like alpha x
+  // scaled afterwards.  Scales beyond the double range take the two-step path.
+  const int sh = 7 * OZ_S - e;
+  const bool direct = e != EXP_NONE && sh < 1000;
+  const double sc = direct ? ldexp(fabs(S.alpha), sh) : 0.0;
+  const bool aneg = S.alpha < 0.0;
+  uint32_t w[OZ_S][4];
+#pragma unroll
+  for (int g4 = 0; g4 < 4; ++g4) {
+    uint32_t hw[4], lw[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const double x = xs[4 * g4 + i];
+      unsigned long long U;
+      if (direct) {
+        U = __double2ull_rz(fabs(x) * sc);
+      } else {
+        U = (e == EXP_NONE) ? 0ull : __double2ull_rz(ldexp(fabs(x * S.alpha), sh));
+      }
+      const uint32_t hi = (uint32_t)(U >> 21), lo = (uint32_t)U & 0x1FFFFFu;
+      uint32_t H = (hi & 0x7Fu) | ((hi << 1) & 0x7F00u) | ((hi << 2) & 0x7F0000u) | ((hi << 3) & 0x7F000000u);
+      uint32_t Lw = (lo & 0x7Fu) | ((lo << 1) & 0x7F00u) | ((lo << 2) & 0x7F0000u);
+      if ((x < 0.0) != aneg) {
+        H = __vneg4(H);
+        Lw = __vneg4(Lw);
+      }
+      hw[i] = H;
+      lw[i] = Lw;
+    }
+    uint32_t th[4], tl[4];
+    transpose4(hw, th);
+    transpose4(lw, tl);
+    // H byte b holds digit 3 - b, Lw byte b digit 6 - b
+    w[0][g4] = th[3];
+    w[1][g4] = th[2];
+    w[2][g4] = th[1];
+    w[3][g4] = th[0];
+    w[4][g4] = tl[2];
+    w[5][g4] = tl[1];
+    w[6][g4] = tl[0];
+  }
+  const int kt = kc >> 1, c = kc & 1, rb = rg >> 6, rr = rg & 63;
+  const size_t off = (size_t)rr * 32 + ((size_t)(c ^ ((rr >> 2) & 1)) << 4);
+#pragma unroll
+  for (int p = 0; p < OZ_S; ++p) {
+    int8_t* dst = S.out + (((size_t)p * S.KT + kt) * RB + rb) * IMG + off;
+    *reinterpret_cast<uint4*>(dst) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
   }
 }
 
-// One thread per 16-byte chunk (row r, k = 16c .. 16c + 15) for all OZ_S
-// digits; K-contiguous operands map consecutive threads along k, the others
-// along rows, so the FP64 reads coalesce.
-__global__ void __launch_bounds__(256) slice_kernel(const __grid_constant__ SliceBatch B) {
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < B.chunks; q += gridDim.x * blockDim.x) {
-    const SliceJob& J = B.job[find_job(B, q, false)];
-    const int local = q - J.chunk_start;
-    const int nrow = J.RB * 64, nkc = 2 * J.KT;
-    int r, kc;
-    if (J.kcontig) {
-      r = local / nkc;
-      kc = local - r * nkc;
-    } else {
-      kc = local / nrow;
-      r = local - kc * nrow;
-    }
-    const int k0 = kc * 16;
-    const int e = r < J.rows ? max(J.exps[r], EXP_NONE) : EXP_NONE;
-    uint32_t w[OZ_S][4];
+// A CTA per unit of SU image rows of one group: the rows' maxima over all
+// segments, their exponents, then the digits of every segment.
+__global__ void __launch_bounds__(SLICE_THREADS, 4) slice_kernel(const __grid_constant__ SliceBatch B) {
+  constexpr int NW = SLICE_THREADS / 32;
+  __shared__ double red[NW][32];
+  __shared__ int ex[SU];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int u = blockIdx.x; u < B.units; u += gridDim.x) {
+    int gi = 0;
+    while (gi + 1 < B.count && u >= B.g[gi + 1].unit_start) ++gi;
+    const SliceGroup& G = B.g[gi];
+    const int r0 = (u - G.unit_start) * SU;
+    double m = 0.0;  // row max (thread r < SU)
+    for (int si = 0; si < G.nseg; ++si) {
+      const SliceSeg& S = G.s[si];
+      double ms = 0.0;
+      if (S.kcontig) {
+        // a row per SLICE_THREADS / SU threads (whole warps), 16-byte loads along k
+        constexpr int TPR = SLICE_THREADS / SU;
+        const int r = tid / TPR, sub = tid % TPR, rg = r0 + r;
+        if (rg < G.rows) {
+          const double* row = S.P + (size_t)rg * S.ld;
+          if (((S.ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(S.P) & 15) == 0)) {
+            int k = 2 * sub;
+#pragma unroll 4
+            for (; k + 1 < S.K; k += 2 * TPR) {
+              const double2 v = *reinterpret_cast<const double2*>(row + k);
+              ms = fmax(ms, fmax(fabs(v.x), fabs(v.y)));
+            }
+            if (k < S.K) ms = fmax(ms, fabs(row[k]));
+          } else {
+            for (int k = sub; k < S.K; k += TPR) ms = fmax(ms, fabs(row[k]));
+          }
+        }
 #pragma unroll
-    for (int p = 0; p < OZ_S; ++p)
+        for (int o = (TPR < 32 ? TPR : 32) / 2; o > 0; o >>= 1) ms = fmax(ms, __shfl_xor_sync(0xffffffffu, ms, o));
+        red[warp][lane] = ms;  // every thread of a row (or of a warp of it) holds its maximum
+        __syncthreads();
+        if (tid < SU) {
+          double v = 0.0;
+          if (TPR >= 32) {
+            for (int w = tid * (TPR / 32); w < (tid + 1) * (TPR / 32); ++w) v = fmax(v, red[w][0]);
+          } else {
+            v = red[(tid * TPR) / 32][(tid * TPR) % 32];
+          }
+          m = fmax(m, fabs(S.alpha) * v);
+        }
+        __syncthreads();
+      } else {
+        // column c = tid % SU of the unit, k phases tid / SU
+        constexpr int KP = SLICE_THREADS / SU;
+        const int c = tid % SU, ph = tid / SU, rg = r0 + c;
+        if (rg < G.rows) {
+          const double* col = S.P + rg;
+          int k = ph;
+          for (; k + 7 * KP < S.K; k += 8 * KP) {  // eight independent loads in flight
+            double v[8];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) w[p][i] = 0u;
-    double xs[16];
-    if (J.kcontig && r < J.rows && k0 + 15 < J.K && ((J.ld & 1) == 0) &&
-        ((reinterpret_cast<uintptr_t>(J.P) & 15) == 0)) {
-      const double2* src = reinterpret_cast<const double2*>(J.P + (size_t)r * J.ld + k0);
+            for (int j = 0; j < 8; ++j) v[j] = col[(size_t)(k + j * KP) * S.ld];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const double2 v = src[j];
-        xs[2 * j] = v.x;
-        xs[2 * j + 1] = v.y;
+            for (int j = 0; j < 8; ++j) ms = fmax(ms, fabs(v[j]));
+          }
+          for (; k < S.K; k += KP) ms = fmax(ms, fabs(col[(size_t)k * S.ld]));
+        }
+#pragma unroll
+        for (int o = SU; o < 32; o <<= 1) ms = fmax(ms, __shfl_xor_sync(0xffffffffu, ms, o));
+        if (lane < SU) red[warp][lane] = ms;
+        __syncthreads();
+        if (tid < SU) {
+          double v = 0.0;
+#pragma unroll
+          for (int w = 0; w < NW; ++w) v = fmax(v, red[w][tid]);
+          m = fmax(m, fabs(S.alpha) * v);
+        }
+        __syncthreads();
       }
-    } else {
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int k = k0 + j;
-        xs[j] = (r < J.rows && k < J.K) ? J.P[J.kcontig ? (size_t)r * J.ld + k : (size_t)k * J.ld + r] : 0.0;
+    }
+    if (tid < SU) {
+      const int e = exponent_of(m);
+      ex[tid] = e;
+      if (r0 + tid < G.rows) G.exps[r0 + tid] = e;
+    }
+    __syncthreads();
+    // digits: chunk (row r, 16-k chunk kc), consecutive threads along k for
+    // kcontig segments, along rows otherwise (coalesced FP64 reads)
+    for (int si = 0; si < G.nseg; ++si) {
+      const SliceSeg& S = G.s[si];
+      const int nkc = 2 * S.KT;
+      for (int q = tid; q < SU * nkc; q += SLICE_THREADS) {
+        int r, kc;
+        if (S.kcontig) {
+          r = q / nkc;
+          kc = q - r * nkc;
+        } else {
+          kc = q / SU;
+          r = q - kc * SU;
+        }
+        const int rg = r0 + r;
+        const bool rowok = rg < G.rows;
+        cut_chunk(S, G.RB, rg, rowok, kc, rowok ? max(ex[r], EXP_NONE) : EXP_NONE);
       }
     }
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const double x = xs[j] * J.alpha;
-      const unsigned long long U = __double2ull_rz(ldexp(fabs(x), 7 * OZ_S - e));
-      const bool neg = x < 0.0;
-#pragma unroll
-      for (int p = 0; p < OZ_S; ++p) {
-        int dgt = (int)((U >> (7 * (OZ_S - 1 - p))) & 127ull);
-        if (neg) dgt = -dgt;
-        w[p][j >> 2] |= ((uint32_t)(uint8_t)(int8_t)dgt) << (8 * (j & 3));
-      }
-    }
-    const int kt = kc >> 1, c = kc & 1, rb = r >> 6, rr = r & 63;
-    const size_t off = (size_t)rr * 32 + ((size_t)(c ^ ((rr >> 2) & 1)) << 4);
-#pragma unroll
-    for (int p = 0; p < OZ_S; ++p) {
-      int8_t* dst = J.out + (((size_t)p * J.KT + kt) * J.RB + rb) * IMG + off;
-      *reinterpret_cast<uint4*>(dst) = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
-    }
+    __syncthreads();  // ex and red are reused by the next unit
   }
 }
 
@@ -458,13 +559,6 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
 
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
-struct OpPlan {
-  const double* P;
-  int ld, rows, K, kcontig, RB, KT;
-  double alpha;
-  int* exps;
-  int8_t* out;
-};
 
 }  // namespace
 
@@ -494,7 +588,7 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
     attr_set = true;
   }
   uint8_t* w = static_cast<uint8_t*>(ws);
-  std::vector<OpPlan> ops;
+  std::vector<SliceGroup> groups;
   std::vector<QProb> qp;
   for (const GemmProb& p : probs) {
     if (p.M <= 0 || p.N <= 0) continue;
@@ -515,9 +609,15 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
     w += align256((size_t)p.N * 4);
     q.eA = eA;
     q.fB = fB;
-    // row / column maxima combine by atomicMax from the lowest int
-    if (cudaMemsetAsync(eA, 0x80, (size_t)p.M * 4, stream) != cudaSuccess) return cudaErrorUnknown;
-    if (cudaMemsetAsync(fB, 0x80, (size_t)p.N * 4, stream) != cudaSuccess) return cudaErrorUnknown;
+    SliceGroup ga{}, gb{};
+    ga.exps = eA;
+    ga.rows = p.M;
+    ga.RB = 2 * q.tmn;
+    ga.nseg = p.nseg;
+    gb.exps = fB;
+    gb.rows = p.N;
+    gb.RB = q.tnn;
+    gb.nseg = p.nseg;
     for (int s = 0; s < p.nseg; ++s) {
       const GemmSeg& g = p.seg[s];
       const int KT = (g.K + QBK - 1) / QBK;
@@ -526,48 +626,31 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
       w += align256((size_t)OZ_S * KT * RBa * IMG);
       int8_t* db = reinterpret_cast<int8_t*>(w);
       w += align256((size_t)OZ_S * KT * RBb * IMG);
-      ops.push_back({g.A, g.lda, p.M, g.K, (g.flags & GF_A_T) ? 0 : 1, RBa, KT, g.alpha, eA, da});
-      ops.push_back({g.B, g.ldb, p.N, g.K, (g.flags & GF_B_KN) ? 0 : 1, RBb, KT, 1.0, fB, db});
+      ga.s[s] = SliceSeg{g.A, da, g.alpha, g.lda, g.K, (g.flags & GF_A_T) ? 0 : 1, KT};
+      gb.s[s] = SliceSeg{g.B, db, 1.0, g.ldb, g.K, (g.flags & GF_B_KN) ? 0 : 1, KT};
       q.seg[s] = QSeg{da, db, KT, RBa, RBb, g.flags, g.K};
     }
+    groups.push_back(ga);
+    groups.push_back(gb);
     qp.push_back(q);
   }
-  // exponents, then digits (every exponent of a problem is final before its
-  // operands are cut)
-  for (int pass = 0; pass < 2; ++pass) {
+  // exponents and digits, SU image rows of a problem side per unit
+  {
     size_t i = 0;
-    while (i < ops.size()) {
+    while (i < groups.size()) {
       SliceBatch sb;
       std::memset(&sb, 0, sizeof(sb));
-      int units = 0, chunks = 0;
-      for (; i < ops.size() && sb.count < SLICE_MAXJ; ++i) {
-        const OpPlan& o = ops[i];
-        SliceJob& J = sb.job[sb.count++];
-        J.P = o.P;
-        J.alpha = o.alpha;
-        J.exps = o.exps;
-        J.out = o.out;
-        J.ld = o.ld;
-        J.rows = o.rows;
-        J.K = o.K;
-        J.kcontig = o.kcontig;
-        J.RB = o.RB;
-        J.KT = o.KT;
-        J.unit_start = units;
-        J.chunk_start = chunks;
-        units += ((o.rows + 31) / 32) * std::max(1, (o.K + EXP_KCHUNK - 1) / EXP_KCHUNK);
-        chunks += o.RB * 64 * 2 * o.KT;
+      int units = 0;
+      for (; i < groups.size() && sb.count < SLICE_MAXG; ++i) {
+        SliceGroup g = groups[i];
+        g.unit_start = units;
+        units += g.RB * (64 / SU);
+        sb.g[sb.count++] = g;
       }
       sb.units = units;
-      sb.chunks = chunks;
+      if (units == 0) continue;
       bta::ProfScope _ps(bta::PROF_SLICE, stream);
-      if (pass == 0) {
-        const int grid = std::max(1, std::min((units * 32 + 255) / 256, 148 * 16));
-        slice_exp_kernel<<<grid, 256, 0, stream>>>(sb);
-      } else {
-        const int grid = std::max(1, std::min((chunks + 255) / 256, 148 * 16));
-        slice_kernel<<<grid, 256, 0, stream>>>(sb);
-      }
+      slice_kernel<<<units, SLICE_THREADS, 0, stream>>>(sb);
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return e;
     }
