@@ -39,12 +39,14 @@ namespace {
 constexpr int OZ_S = 7;                        // digits per operand
 constexpr int QBM = 128, QBN = 64, QBK = 32;   // output tile, k-slab (32 int8 = one 32-byte row)
 constexpr int IMG = 64 * QBK;                  // one 64-row digit image (2 KB)
-constexpr int QSTAGES = 4;
+constexpr int QSTAGES = 3;
 constexpr int A_SLICE = 2 * IMG;               // 128 rows
 constexpr int B_SLICE = IMG;                   // 64 rows
 constexpr int QSTAGE_BYTES = OZ_S * (A_SLICE + B_SLICE);
 constexpr int QTHREADS = 6 * 32;               // 4 epilogue warps, producer warp, MMA warp
-constexpr size_t QSMEM_BYTES = size_t(QSTAGES) * QSTAGE_BYTES + 256 + 1024;
+constexpr int QSTAGE_LD = 65;                  // epilogue staging: 32 rows x 64 columns per warp, padded
+constexpr int QEPI_BYTES = 4 * 32 * QSTAGE_LD * 8;
+constexpr size_t QSMEM_BYTES = size_t(QSTAGES) * QSTAGE_BYTES + QEPI_BYTES + 256 + 1024;
 constexpr int TMEM_COLS = 512;                 // OZ_S accumulators of QBN columns
 constexpr long long QWAIT_CYCLES = 4000000000LL;
 constexpr int EXP_NONE = -1100;                // exponent of an all-zero row
@@ -58,6 +60,11 @@ __host__ __device__ constexpr uint32_t idesc_i8(int n) {
 constexpr int QMMA_NMAX = 256;  // largest N of one M = 128 MMA
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Exact double of an integer |n| < 2^51: the bits of 1.5 2^52 + n, minus 1.5 2^52.
+__device__ __forceinline__ double exact_double(long long n) {
+  return __longlong_as_double(0x4338000000000000LL + n) - 6755399441055744.0;
+}
 
 // K-major operand in the 32-byte swizzle layout: rows of 32 bytes, 8-row
 // groups 256 bytes apart, descriptor version 1, layout type 6 (SWIZZLE_32B).
@@ -120,21 +127,27 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
       : "memory");
 }
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, int (&v)[32]) {
-  uint32_t r[32];
+// 16 columns of the warp's 32 lanes, asynchronous: the registers are valid
+// after tmem_wait16().
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 32; ++i) v[i] = (int)r[i];
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
 }
+// Waits for the outstanding tensor-memory loads; r (the destination of the
+// last one) is an operand so no read of it moves above the wait.
+__device__ __forceinline__ void tmem_wait16(uint32_t (&r)[16]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                 "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+               :
+               : "memory");
+}
+
 
 // ---------------------------------------------------------------- slicing
 // One side of one problem: the op(A) (or op(B)) operands of its segments,
@@ -403,20 +416,13 @@ __device__ __forceinline__ int qseg_range(const QSeg& s, int m0, int n0, int& kt
   return kt1 > kt0 ? kt1 - kt0 : 0;
 }
 
-__global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_constant__ QBatch batch, int* abort_flag) {
-  extern __shared__ uint8_t smem_raw[];
-  uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
-  uint8_t* bars = smem + QSTAGES * QSTAGE_BYTES;
-  const uint32_t full0 = smem_u32(bars), empty0 = full0 + 8 * QSTAGES, done_bar = empty0 + 8 * QSTAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 8 * (2 * QSTAGES + 1));
-
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int bid = blockIdx.x;
-  int pi = 0;
-  while (pi + 1 < batch.count && bid >= batch.tile_start[pi + 1]) ++pi;
+// Tile t of a batch: problem, tile row, tile column.
+__device__ __forceinline__ void decode_tile(const QBatch& batch, int t, int& pi, int& tm, int& tn) {
+  pi = 0;
+  while (pi + 1 < batch.count && t >= batch.tile_start[pi + 1]) ++pi;
   const QProb& P = batch.p[pi];
-  int local = bid - batch.tile_start[pi];
-  int tm = 0, tn = 0;
+  int local = t - batch.tile_start[pi];
+  tm = 0;
   if (P.cflags & GC_LOWER) {
     while (local >= lower_tiles_row(tm, P.tnn)) local -= lower_tiles_row(tm++, P.tnn);
     tn = local;
@@ -424,7 +430,32 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
     tm = local / P.tnn;
     tn = local - tm * P.tnn;
   }
-  const int m0 = tm * QBM, n0 = tn * QBN;
+}
+
+__device__ __forceinline__ int tile_steps(const QProb& P, int m0, int n0) {
+  int nsteps = 0;
+  for (int si = 0; si < P.nseg; ++si) {
+    int kt0;
+    nsteps += qseg_range(P.seg[si], m0, n0, kt0);
+  }
+  return nsteps;
+}
+
+// Persistent: CTA c takes tiles c, c + grid, ...  The producer's ring runs
+// across tile boundaries; the MMA warp starts a tile once the epilogue has
+// read the previous tile's accumulators out of tensor memory (tmem_empty), so
+// the epilogue's scaling and stores overlap the next tile's products.
+__global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_constant__ QBatch batch, int total_tiles,
+                                                               int* abort_flag) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+  double* epi_stage = reinterpret_cast<double*>(smem + QSTAGES * QSTAGE_BYTES);
+  uint8_t* bars = smem + QSTAGES * QSTAGE_BYTES + QEPI_BYTES;
+  const uint32_t full0 = smem_u32(bars), empty0 = full0 + 8 * QSTAGES, done_bar = empty0 + 8 * QSTAGES;
+  const uint32_t tmem_empty = done_bar + 8, drain_bar = done_bar + 16;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 8 * (2 * QSTAGES + 3));
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (warp == 5) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -438,18 +469,14 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
       mbar_init(empty0 + 8 * s, 1);
     }
     mbar_init(done_bar, 1);
+    mbar_init(tmem_empty, 4);  // one arrival per epilogue warp
+    mbar_init(drain_bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-
-  int nsteps = 0;
-  for (int si = 0; si < P.nseg; ++si) {
-    int kt0;
-    nsteps += qseg_range(P.seg[si], m0, n0, kt0);
-  }
   const uint32_t stage0 = smem_u32(smem);
 
   if (warp == 4) {
@@ -457,25 +484,30 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
     if (lane == 0) {
       int step = 0;
       bool ok = true;
-      for (int si = 0; si < P.nseg && ok; ++si) {
-        const QSeg& s = P.seg[si];
-        int kt0;
-        const int nk = qseg_range(s, m0, n0, kt0);
-        for (int i = 0; i < nk; ++i, ++step) {
-          const int st = step % QSTAGES;
-          if (step >= QSTAGES && !mbar_wait(empty0 + 8 * st, ((step / QSTAGES) - 1) & 1, abort_flag)) {
-            ok = false;
-            break;
-          }
-          const int kt = kt0 + i;
-          const uint32_t bar = full0 + 8 * st;
-          mbar_expect_tx(bar, QSTAGE_BYTES);
-          const uint32_t dst = stage0 + st * QSTAGE_BYTES;
+      for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
+        int pi, tm, tn;
+        decode_tile(batch, t, pi, tm, tn);
+        const QProb& P = batch.p[pi];
+        for (int si = 0; si < P.nseg && ok; ++si) {
+          const QSeg& sg = P.seg[si];
+          int kt0;
+          const int nk = qseg_range(sg, tm * QBM, tn * QBN, kt0);
+          for (int i = 0; i < nk; ++i, ++step) {
+            const int st = step % QSTAGES;
+            if (step >= QSTAGES && !mbar_wait(empty0 + 8 * st, ((step / QSTAGES) - 1) & 1, abort_flag)) {
+              ok = false;
+              break;
+            }
+            const int kt = kt0 + i;
+            const uint32_t bar = full0 + 8 * st;
+            mbar_expect_tx(bar, QSTAGE_BYTES);
+            const uint32_t dst = stage0 + st * QSTAGE_BYTES;
 #pragma unroll
-          for (int p = 0; p < OZ_S; ++p) {
-            bulk_g2s(dst + p * A_SLICE, s.A + (((size_t)p * s.KT + kt) * s.RBa + 2 * tm) * IMG, A_SLICE, bar);
-            bulk_g2s(dst + OZ_S * A_SLICE + p * B_SLICE, s.B + (((size_t)p * s.KT + kt) * s.RBb + tn) * IMG,
-                     B_SLICE, bar);
+            for (int p = 0; p < OZ_S; ++p) {
+              bulk_g2s(dst + p * A_SLICE, sg.A + (((size_t)p * sg.KT + kt) * sg.RBa + 2 * tm) * IMG, A_SLICE, bar);
+              bulk_g2s(dst + OZ_S * A_SLICE + p * B_SLICE, sg.B + (((size_t)p * sg.KT + kt) * sg.RBb + tn) * IMG,
+                       B_SLICE, bar);
+            }
           }
         }
       }
@@ -483,74 +515,154 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
   } else if (warp == 5) {
     // ------------------------------------------------------ MMA issuer
     if (lane == 0) {
-      for (int step = 0; step < nsteps; ++step) {
-        const int st = step % QSTAGES;
-        if (!mbar_wait(full0 + 8 * st, (step / QSTAGES) & 1, abort_flag)) break;
+      int step = 0, it = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x, ++it) {
+        int pi, tm, tn;
+        decode_tile(batch, t, pi, tm, tn);
+        const int nsteps = tile_steps(batch.p[pi], tm * QBM, tn * QBN);
+        // the epilogue has read the previous tile's accumulators
+        if (it > 0 && !mbar_wait(tmem_empty, (it - 1) & 1, abort_flag)) break;
         tc_fence_after();
-        const uint32_t a0 = stage0 + st * QSTAGE_BYTES, b0 = a0 + OZ_S * A_SLICE;
-#pragma unroll
-        for (int p = 0; p < OZ_S; ++p) {
-          // digit p of A against the stacked digit images q = q0 .. q0+nq-1 of
-          // B (consecutive 64-row images form one K-major operand of 64 nq
-          // rows): product (p, q) lands in columns (p + q) QBN .. of tensor
-          // memory, the accumulator of d = p + q.  The first products of the
-          // tile, p = 0 at step 0, overwrite every accumulator.
-          const uint32_t acc = (step > 0 || p > 0) ? 1u : 0u;
-#pragma unroll
-          for (int q0 = 0; q0 < OZ_S - p; q0 += QMMA_NMAX / QBN) {
-            const int nq = min(QMMA_NMAX / QBN, OZ_S - p - q0);
-            mma_i8(tmem + (uint32_t)((p + q0) * QBN), sw32_desc(a0 + p * A_SLICE), sw32_desc(b0 + q0 * B_SLICE),
-                   idesc_i8(nq * QBN), acc);
+        for (int ks = 0; ks < nsteps; ++ks, ++step) {
+          const int st = step % QSTAGES;
+          if (!mbar_wait(full0 + 8 * st, (step / QSTAGES) & 1, abort_flag)) {
+            ok = false;
+            break;
           }
+          tc_fence_after();
+          const uint32_t a0 = stage0 + st * QSTAGE_BYTES, b0 = a0 + OZ_S * A_SLICE;
+#pragma unroll
+          for (int p = 0; p < OZ_S; ++p) {
+            // digit p of A against the stacked digit images q = q0 .. q0+nq-1
+            // of B (consecutive 64-row images form one K-major operand of
+            // 64 nq rows): product (p, q) lands in columns (p + q) QBN .. of
+            // tensor memory, the accumulator of d = p + q.  The first
+            // products of a tile, p = 0 at its first step, overwrite every
+            // accumulator.
+            const uint32_t acc = (ks > 0 || p > 0) ? 1u : 0u;
+#pragma unroll
+            for (int q0 = 0; q0 < OZ_S - p; q0 += QMMA_NMAX / QBN) {
+              const int nq = min(QMMA_NMAX / QBN, OZ_S - p - q0);
+              mma_i8(tmem + (uint32_t)((p + q0) * QBN), sw32_desc(a0 + p * A_SLICE), sw32_desc(b0 + q0 * B_SLICE),
+                     idesc_i8(nq * QBN), acc);
+            }
+          }
+          tc_commit(empty0 + 8 * st);
         }
-        tc_commit(empty0 + 8 * st);
+        tc_commit(done_bar);  // also for a tile without products: the epilogue then writes beta C
       }
-      tc_commit(done_bar);
+      // every product issued has completed before the tensor memory is freed
+      tc_commit(drain_bar);
+      mbar_wait(drain_bar, 0, abort_flag);
     }
   } else {
     // ------------------------------------------------------ epilogue (warps 0-3: rows 32 w .. 32 w + 31)
-    const bool have = __all_sync(0xffffffffu, nsteps > 0 && mbar_wait(done_bar, 0, abort_flag));
-    tc_fence_after();
-    const int row = m0 + 32 * warp + lane;
-    const bool rowok = row < P.M;
-    const int er = rowok ? max(P.eA[row], EXP_NONE) : 0;
-    const bool lower = P.cflags & GC_LOWER;
-    const bool mirror = P.cflags & GC_MIRROR;
-    double* C = P.C;
+    // Per 16 columns: the seven level accumulators combine exactly,
+    // hi = sum_{d<4} acc_d 2^(7(3-d)) (< 2^49) and lo = sum_{d>=4} acc_d
+    // 2^(7(6-d)); C = (hi + lo 2^-21) 2^(e_m + f_n - 35) goes to the warp's
+    // staging rows.  Then the tensor memory is released and the warp writes
+    // whole 256-byte row segments while the next tile's products run.
+    double* stage = epi_stage + warp * (32 * QSTAGE_LD);
+    const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
+    int it = 0;
+    for (int t = blockIdx.x; t < total_tiles; t += gridDim.x, ++it) {
+      int pi, tm, tn;
+      decode_tile(batch, t, pi, tm, tn);
+      const QProb& P = batch.p[pi];
+      const int m0 = tm * QBM, n0 = tn * QBN;
+      const int nsteps = tile_steps(P, m0, n0);
+      if (!__all_sync(0xffffffffu, mbar_wait(done_bar, it & 1, abort_flag))) break;
+      tc_fence_after();
+      const bool have = nsteps > 0;
+      const int row = m0 + 32 * warp + lane;
+      const bool rowok = row < P.M;
+      const int er = rowok ? max(P.eA[row], EXP_NONE) : 0;
 #pragma unroll 1
-    for (int c = 0; c < QBN / 32; ++c) {
-      const int col0 = n0 + 32 * c;
-      double v[32];
+      for (int c = 0; c < QBN / 32; ++c) {
+        const int col0 = n0 + 32 * c;
+        const int fcol = (col0 + lane < P.N) ? max(P.fB[col0 + lane], EXP_NONE) : 0;
 #pragma unroll
-      for (int j = 0; j < 32; ++j) v[j] = 0.0;
-      if (have) {
-#pragma unroll 1
-        for (int d = OZ_S - 1; d >= 0; --d) {
-          int acc[32];
-          tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(d * QBN + 32 * c), acc);
-          const double sc = ldexp(1.0, -7 * (d + 2));
+        for (int h = 0; h < 2; ++h) {
+          long long hi[16], lo[16];
 #pragma unroll
-          for (int j = 0; j < 32; ++j) v[j] += sc * (double)acc[j];
+          for (int j = 0; j < 16; ++j) hi[j] = lo[j] = 0;
+          if (have) {
+            uint32_t ra[16], rb[16];
+            const uint32_t tcol = trow + (uint32_t)(32 * c + 16 * h);
+            tmem_ld16(tcol, ra);
+#pragma unroll
+            for (int d = 0; d < OZ_S; ++d) {
+              uint32_t cur[16];
+              if (d & 1) {
+                tmem_wait16(rb);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) cur[j] = rb[j];
+              } else {
+                tmem_wait16(ra);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) cur[j] = ra[j];
+              }
+              if (d + 1 < OZ_S) {
+                if (d & 1) tmem_ld16(tcol + (uint32_t)((d + 1) * QBN), ra);
+                else tmem_ld16(tcol + (uint32_t)((d + 1) * QBN), rb);
+              }
+#pragma unroll
+              for (int j = 0; j < 16; ++j) {
+                if (d < 4) hi[j] = hi[j] * 128 + (int)cur[j];
+                else lo[j] = lo[j] * 128 + (int)cur[j];
+              }
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int fc = __shfl_sync(0xffffffffu, fcol, 16 * h + j);
+            const double v = fma(exact_double(lo[j]), 0x1p-21, exact_double(hi[j]));
+            const int sh = er + fc - 35;
+            const double x = (sh > -900 && sh < 900) ? v * __longlong_as_double((long long)(sh + 1023) << 52)
+                                                     : ldexp(v, sh);
+            stage[lane * QSTAGE_LD + 32 * c + 16 * h + j] = x;
+          }
         }
       }
-      if (!rowok || col0 >= P.N || (lower && col0 > row)) continue;
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const int col = col0 + j;
-        if (col >= P.N || (lower && col > row)) continue;
-        double x = ldexp(v[j], er + max(P.fB[col], EXP_NONE));
-        double* dst = C + (size_t)row * P.ldc + col;
-        if (P.beta != 0.0) x += P.beta * *dst;
-        *dst = x;
-        if (mirror && col < row) C[(size_t)col * P.ldc + row] = x;
+      // accumulators read: the next tile's products may start
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tmem_empty);
+      const bool lower = P.cflags & GC_LOWER;
+      const bool mirror = P.cflags & GC_MIRROR;
+      double* C = P.C;
+      const int rbase = m0 + 32 * warp;
+#pragma unroll 1
+      for (int c = 0; c < QBN / 32; ++c) {
+        // row segments: lane = column
+        const int col = n0 + 32 * c + lane;
+#pragma unroll 4
+        for (int rr = 0; rr < 32; ++rr) {
+          const int rw = rbase + rr;
+          if (rw < P.M && col < P.N && (!lower || col <= rw)) {
+            double* dst = C + (size_t)rw * P.ldc + col;
+            double x = stage[rr * QSTAGE_LD + 32 * c + lane];
+            if (P.beta != 0.0) x += P.beta * *dst;
+            *dst = x;
+          }
+        }
+        // mirror: lane = row, so the transposed writes are contiguous too
+        if (mirror && rowok) {
+#pragma unroll 4
+          for (int j = 0; j < 32; ++j) {
+            const int cm = n0 + 32 * c + j;
+            if (cm < row && cm < P.N) C[(size_t)cm * P.ldc + row] = stage[lane * QSTAGE_LD + 32 * c + j];
+          }
+        }
       }
+      __syncwarp();
     }
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 5) {
     tc_fence_after();
-    if (nsteps > 0 && lane == 0) mbar_wait(done_bar, 0, abort_flag);
     __syncwarp();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)TMEM_COLS)
                  : "memory");
@@ -674,9 +786,16 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
       b.count++;
     }
     b.tile_start[b.count] = total;
-    {
+    if (total > 0) {
+      static int sms = 0;
+      if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        sms = std::max(1, sms);
+      }
       bta::ProfScope _ps(bta::PROF_GEMM, stream);
-      gemm_i8_kernel<<<total, QTHREADS, QSMEM_BYTES, stream>>>(b, abort_flag);
+      gemm_i8_kernel<<<std::min(total, sms), QTHREADS, QSMEM_BYTES, stream>>>(b, total, abort_flag);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
