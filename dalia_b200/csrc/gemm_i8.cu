@@ -582,6 +582,11 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
       for (int c = 0; c < QBN / 32; ++c) {
         const int col0 = n0 + 32 * c;
         const int fcol = (col0 + lane < P.N) ? max(P.fB[col0 + lane], EXP_NONE) : 0;
+        // exponents in the normal range (every tile of ordinary data): two
+        // exact power-of-two products; otherwise ldexp on a separate path
+        const bool fast = __all_sync(0xffffffffu, er > -900 && er < 900 && fcol > -900 && fcol < 900);
+        const double srow = fast ? __longlong_as_double((long long)(er - 35 + 1023) << 52) : 0.0;
+        const double scol = fast ? __longlong_as_double((long long)(fcol + 1023) << 52) : 0.0;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
           long long hi[16], lo[16];
@@ -614,14 +619,20 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
               }
             }
           }
+          if (fast) {
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int fc = __shfl_sync(0xffffffffu, fcol, 16 * h + j);
-            const double v = fma(exact_double(lo[j]), 0x1p-21, exact_double(hi[j]));
-            const int sh = er + fc - 35;
-            const double x = (sh > -900 && sh < 900) ? v * __longlong_as_double((long long)(sh + 1023) << 52)
-                                                     : ldexp(v, sh);
-            stage[lane * QSTAGE_LD + 32 * c + 16 * h + j] = x;
+            for (int j = 0; j < 16; ++j) {
+              const double sc = __shfl_sync(0xffffffffu, scol, 16 * h + j);
+              const double v = fma(exact_double(lo[j]), 0x1p-21, exact_double(hi[j]));
+              stage[lane * QSTAGE_LD + 32 * c + 16 * h + j] = (v * srow) * sc;
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const int fc = __shfl_sync(0xffffffffu, fcol, 16 * h + j);
+              const double v = fma(exact_double(lo[j]), 0x1p-21, exact_double(hi[j]));
+              stage[lane * QSTAGE_LD + 32 * c + 16 * h + j] = ldexp(v, er + fc - 35);
+            }
           }
         }
       }
