@@ -223,10 +223,15 @@ __device__ __forceinline__ void cut_chunk(const SliceSeg& S, int RB, int rg, boo
     }
   }
   // |alpha| 2^(7 OZ_S - e) is exact; products with it round like alpha x
-  // scaled afterwards.  Scales beyond the double range take the two-step path.
+  // scaled afterwards.  Scales beyond the double range (tiny rows) scale
+  // |alpha x| by 2^(sh - 600) and 2^600, both exact; an all-zero row gets 0.
+  // Every entry takes the same three products (no per-entry branch).
   const int sh = 7 * OZ_S - e;
   const bool direct = e != EXP_NONE && sh < 1000;
-  const double sc = direct ? ldexp(fabs(S.alpha), sh) : 0.0;
+  const double s1 = direct ? ldexp(fabs(S.alpha), sh)
+                           : (e == EXP_NONE ? 0.0 : __longlong_as_double((long long)(sh - 600 + 1023) << 52));
+  const double s2 = direct ? 1.0 : 0x1p600;
+  const double a1 = direct ? 1.0 : S.alpha;
   const bool aneg = S.alpha < 0.0;
   uint32_t w[OZ_S][4];
 #pragma unroll
@@ -235,12 +240,7 @@ __device__ __forceinline__ void cut_chunk(const SliceSeg& S, int RB, int rg, boo
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const double x = xs[4 * g4 + i];
-      unsigned long long U;
-      if (direct) {
-        U = __double2ull_rz(fabs(x) * sc);
-      } else {
-        U = (e == EXP_NONE) ? 0ull : __double2ull_rz(ldexp(fabs(x * S.alpha), sh));
-      }
+      const unsigned long long U = __double2ull_rz((fabs(x * a1) * s1) * s2);
       const uint32_t hi = (uint32_t)(U >> 21), lo = (uint32_t)U & 0x1FFFFFu;
       uint32_t H = (hi & 0x7Fu) | ((hi << 1) & 0x7F00u) | ((hi << 2) & 0x7F0000u) | ((hi << 3) & 0x7F000000u);
       uint32_t Lw = (lo & 0x7Fu) | ((lo << 1) & 0x7F00u) | ((lo << 2) & 0x7F0000u);
