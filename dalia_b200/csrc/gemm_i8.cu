@@ -172,7 +172,7 @@ struct SliceGroup {
 
 constexpr int SLICE_MAXG = 48;
 constexpr int SLICE_THREADS = 256;
-constexpr int SU = 32;  // image rows per slicing unit
+constexpr int SU = 16;  // image rows per slicing unit
 
 struct SliceBatch {
   int count;
