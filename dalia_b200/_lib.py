@@ -66,6 +66,7 @@ SIGNATURES = {
     "bta_noalloc_scratch_bytes": (ctypes.c_size_t, []),
     "bta_prof_enable": (_int, [_int]),
     "bta_prof_read": (_int, [_pdbl, ctypes.POINTER(ctypes.c_longlong)]),
+    "bta_panel_task_list": (_int, [_int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _int, ctypes.POINTER(_int)]),
     "bta_gather_coo": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _i64, _int,
                               _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p]),
     "bta_scatter_coo": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _i64, _int,

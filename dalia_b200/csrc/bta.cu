@@ -553,6 +553,39 @@ int bta_pobtasi(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, doub
   return bta_pobtasi_batched(h, 1, &n, &b, &a, &D, &L, &Ab, &T);
 }
 
+int bta_panel_task_list(int count, const int* b, const int* a, const int* flags, int* out, int cap, int* n_out) {
+  if (count < 1 || count > PANEL_MAXI || !b || !a || !flags || !n_out || cap < 0 || (cap > 0 && !out))
+    return BTA_ERR_INVALID;
+  static double present;  // stands for a matrix block: only null / non-null matters here
+  std::vector<PanelInst> insts;
+  for (int k = 0; k < count; ++k) {
+    if (b[k] < 1 || a[k] < 0) return BTA_ERR_INVALID;
+    const bool hasL = flags[k] & 1;
+    PanelInst I{};
+    I.b = b[k];
+    I.a = a[k];
+    I.nq = (b[k] + 63) / 64;
+    I.L = hasL ? &present : nullptr;
+    I.Ab = a[k] > 0 ? &present : nullptr;
+    I.Lprev = (flags[k] & 2) ? &present : nullptr;
+    I.Abprev = ((flags[k] & 4) && a[k] > 0) ? &present : nullptr;
+    I.Ttip = ((flags[k] & 8) && a[k] > 0 && a[k] <= 64) ? &present : nullptr;
+    I.nrows_t = panel_rows(b[k], a[k], hasL);
+    insts.push_back(I);
+  }
+  std::vector<int4> t;
+  panel_tasks(insts, t);
+  *n_out = (int)t.size();
+  if ((int)t.size() > cap) return BTA_ERR_INVALID;
+  for (size_t i = 0; i < t.size(); ++i) {
+    out[4 * i] = t[i].x;
+    out[4 * i + 1] = t[i].y;
+    out[4 * i + 2] = t[i].z;
+    out[4 * i + 3] = t[i].w;
+  }
+  return BTA_OK;
+}
+
 int bta_block_inverses(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const double* const* D,
                        double* const* V) {
   if (!h || count < 1 || !n || !b || !D || !V) return BTA_ERR_INVALID;

@@ -220,6 +220,19 @@ long long bta_launch_count(void);
 int bta_prof_enable(int on);
 int bta_prof_read(double* ms, long long* counts);
 
+/*
+ * Task queue of one block-column launch of the factorisation, for tests of
+ * its order (no counterpart in the reference).  For count matrices (at most
+ * 64) with block size b[k], arrow size a[k] and flags[k] (bit 0: a block
+ * below the diagonal block, bit 1: the previous block column's Schur term,
+ * bit 2: the previous arrow block, bit 3: the arrow tip), writes up to cap
+ * tasks {matrix, kind, tile row, tile column} as four ints each to out and
+ * their number to *n_out (kinds: 3 diagonal tile, 4 tile below it, 5 tile with
+ * its triangular solve, 6 arrow tip, 7 previous-column term).  Host code only:
+ * needs no device.  BTA_ERR_INVALID when cap is too small.
+ */
+int bta_panel_task_list(int count, const int* b, const int* a, const int* flags, int* out, int cap, int* n_out);
+
 #ifdef __cplusplus
 }
 #endif
