@@ -8,23 +8,26 @@
 // 7-bit digits (truncation: |x 2^-e - sum_p a_p 2^-7p| < 2^-7 OZ_S).  Then
 //   C[m][n] = beta C + 2^(e_m + f_n) sum_{d} 2^-7d sum_{p+q=d} (a_p . b_q)
 // where every digit product sum is exact in INT32 (|a_p b_q| <= 127^2, at
-// most OZ_S pairs per d, K <= 19000).  Keeping d <= OZ_S + 1 drops terms
-// below 2^-7(OZ_S+1) 127^2 per element product: a relative error of ~1e-14
-// against sum_k |a||b| for OZ_S = 7.  Seven digits are needed because the
+// most OZ_S pairs per d, K <= 19000).  Keeping the pairs with p + q <= OZ_S - 1
+// (28 of 49, digits counted from 0) drops products below 2^-7(OZ_S+2) 127^2
+// per element product: a relative error of ~1e-14 against sum_k |a||b| for
+// OZ_S = 7.  Seven digits are needed because the
 // selected inversion of an ill-conditioned precision (cond ~1e9 per block)
 // amplifies the truncation: five digits left gradient errors of 2e-3 at
 // b = 1500.
 //
-// Pipeline: slice_kernel (per 32 rows of a problem side: the maxima over all
+// Pipeline: slice_kernel (per 16 rows of a problem side: the maxima over all
 // segments -> exponents, then the digits, written as the 32-byte-swizzled
-// K-major shared-memory images the MMA reads), gemm_i8_kernel: one producer thread bulk-copies the
-// digit images of a 32-wide k-slab (A: 128 rows x OZ_S digits, B: 64 rows x
-// OZ_S digits, no multicast) into a 4-stage ring; one thread issues the
-// products of the slab, one MMA per A digit p against the stacked B digits
-// (N up to 256: 10 MMAs for 28 digit pairs), each pair (p, q) landing in the
-// TMEM accumulator of d = p + q; four
-// epilogue warps read the OZ_S accumulators (tcgen05.ld), rescale and write C
-// in FP64.  Every wait is bounded and raises the abort flag on timeout.
+// K-major shared-memory images the MMA reads) and gemm_i8_kernel, persistent
+// CTAs over 128 x 64 output tiles: one producer thread bulk-copies the digit
+// images of each 32-wide k-slab (A: 128 rows x OZ_S digits, B: 64 rows x OZ_S
+// digits, no multicast) into a 3-stage ring; one thread issues the products
+// of the slab, one MMA per A digit p against the stacked B digits (N up to
+// 256: 10 MMAs for 28 digit pairs), each pair (p, q) landing in the TMEM
+// accumulator of d = p + q; four epilogue warps read the OZ_S accumulators
+// (tcgen05.ld), combine them exactly, scale, release the tensor memory to
+// the next tile and write C in FP64 through a shared-memory stage.  Every
+// wait is bounded and raises the abort flag on timeout.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
