@@ -65,6 +65,7 @@ SIGNATURES = {
     "bta_pobtaf_noalloc": (_int, [_i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _pi64, _c_void_p]),
     "bta_noalloc_scratch_bytes": (ctypes.c_size_t, []),
     "bta_prof_enable": (_int, [_int]),
+    "bta_prof_mask": (_int, [_int]),
     "bta_prof_read": (_int, [_pdbl, ctypes.POINTER(ctypes.c_longlong)]),
     "bta_panel_task_list": (_int, [_int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _int, ctypes.POINTER(_int)]),
     "bta_gather_coo": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _i64, _int,

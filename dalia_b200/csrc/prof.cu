@@ -16,6 +16,7 @@ struct Pending {
 
 std::atomic<long long> g_launches{0};
 std::atomic<bool> g_on{false};
+std::atomic<int> g_mask{0xFF};  // categories that get events
 std::mutex g_mu;
 std::vector<Pending> g_pending;
 std::vector<cudaEvent_t> g_pool;
@@ -36,10 +37,9 @@ cudaEvent_t take_event() {
 }  // namespace
 
 void prof_begin(int cat, cudaStream_t s, cudaEvent_t* ev) {
-  (void)cat;
   g_launches.fetch_add(1, std::memory_order_relaxed);
   *ev = nullptr;
-  if (!g_on.load(std::memory_order_relaxed)) return;
+  if (!g_on.load(std::memory_order_relaxed) || !((g_mask.load(std::memory_order_relaxed) >> cat) & 1)) return;
   std::lock_guard<std::mutex> lk(g_mu);
   *ev = take_event();
   cudaEventRecord(*ev, s);
@@ -60,7 +60,22 @@ extern "C" {
 long long bta_launch_count(void) { return bta::g_launches.load(); }
 
 int bta_prof_enable(int on) {
+  if (on) {
+    // events for ~8000 launches made now, so that timing a region costs no
+    // event creation inside it (events return to the pool on bta_prof_read)
+    std::lock_guard<std::mutex> lk(bta::g_mu);
+    while (bta::g_pool.size() < 16384) {
+      cudaEvent_t e = nullptr;
+      if (cudaEventCreate(&e) != cudaSuccess) return BTA_ERR_CUDA;
+      bta::g_pool.push_back(e);
+    }
+  }
   bta::g_on.store(on != 0);
+  return BTA_OK;
+}
+
+int bta_prof_mask(int mask) {
+  bta::g_mask.store(mask);
   return BTA_OK;
 }
 

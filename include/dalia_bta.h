@@ -212,12 +212,17 @@ size_t bta_noalloc_scratch_bytes(void);
  * kernels): total kernel launches of this library in the process, and
  * optional per-category device time from CUDA events recorded around every
  * launch on its stream.  Categories: 0 panel factorisation, 1 GEMM, 2 solve
- * sweeps, 3 block inverses, 4 other.  bta_prof_read synchronises on the
+ * sweeps, 3 block inverses, 4 other.  bta_prof_enable(1) creates the
+ * events beforehand (for about 8000 launches), so a timed region pays no
+ * event creation; bta_prof_mask limits the events to the categories whose
+ * bits are set (default: all), since events around every launch slow a step
+ * of many small launches measurably.  bta_prof_read synchronises on the
  * recorded events, returns the accumulated milliseconds and launch counts
  * (8 entries each) and clears them.
  */
 long long bta_launch_count(void);
 int bta_prof_enable(int on);
+int bta_prof_mask(int mask);
 int bta_prof_read(double* ms, long long* counts);
 
 /*
