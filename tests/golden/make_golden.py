@@ -73,7 +73,20 @@ def _save_hessian(name, th, dal):
     print(f"hess_{name}: diag={np.diag(np.asarray(h))}", flush=True)
 
 
-def main(ref_root: str, only=None, hessian=False) -> None:
+def _save_minimize(name, th, dal):
+    """min_<name>.npz: DALIA.minimize from theta (Serinv path, the reference's
+    default BFGSConfig and early-exit settings, FD gradient)."""
+    r = dal.minimize()
+    out = {"theta0": th, "theta": np.asarray(r["theta"], dtype=np.float64), "f": np.array(r["f"]),
+           "f_values": np.asarray(r["f_values"], dtype=np.float64),
+           "theta_values": np.asarray(r["theta_values"], dtype=np.float64),
+           "grad_f": np.asarray(r["grad_f"], dtype=np.float64), "x": np.asarray(r["x"], dtype=np.float64)}
+    np.savez_compressed(os.path.join(HERE, f"min_{name}.npz"), **out)
+    print(f"min_{name}: theta*={out['theta']} f*={float(out['f']):.10f} iterations={len(out['f_values'])}",
+          flush=True)
+
+
+def main(ref_root: str, only=None, hessian=False, minimize=False) -> None:
     os.environ.setdefault("ARRAY_MODULE", "numpy")
     sys.path.insert(0, REPO)
     sys.path.insert(0, os.path.join(ref_root, "src"))
@@ -152,6 +165,9 @@ def main(ref_root: str, only=None, hessian=False) -> None:
         th = np.asarray(theta, dtype=np.float64)
         if hessian:
             _save_hessian(name, th, build("serinv")[1])
+            continue
+        if minimize:
+            _save_minimize(name, th, build("serinv")[1])
             continue
 
         # --- dense solver: exact reference numbers
@@ -292,11 +308,16 @@ def main_coregional(ref_root: str, only=None, hessian=False) -> None:
 
 
 if __name__ == "__main__":
-    # usage: make_golden.py [REF_ROOT [--hessian] [CASE ...]]
-    #   --hessian writes hess_<CASE>.npz (the reference's FD Hessian) instead
+    # usage: make_golden.py [REF_ROOT [--hessian | --minimize] [CASE ...]]
+    #   --hessian writes hess_<CASE>.npz (the reference's FD Hessian) instead,
+    #   --minimize writes min_<CASE>.npz (the reference's DALIA.minimize)
     _root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DALIA_REF", "/root/reference")
     _hess = "--hessian" in sys.argv[2:]
-    _only = [a for a in sys.argv[2:] if a != "--hessian"]
+    _min = "--minimize" in sys.argv[2:]
+    _only = [a for a in sys.argv[2:] if a not in ("--hessian", "--minimize")]
+    if _min:
+        main(_root, [c for c in _only if c in CASES], minimize=True)
+        sys.exit(0)
     if not _only or any(c in CASES for c in _only):
         main(_root, [c for c in _only if c in CASES], hessian=_hess)
     if not _only or any(c in COREG_CASES for c in _only):
