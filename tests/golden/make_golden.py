@@ -225,7 +225,7 @@ def coreg_checksums(prob):
     return out
 
 
-def main_coregional(ref_root: str, only=None, hessian=False) -> None:
+def main_coregional(ref_root: str, only=None, hessian=False, minimize=False) -> None:
     """Coregional fixtures: the reference's ``CoregionalModel`` built from one
     ``Model`` per variate (Gaussian priors as in its coregional examples),
     driven through ``DALIA._objective_function`` with the dense and the
@@ -289,6 +289,9 @@ def main_coregional(ref_root: str, only=None, hessian=False) -> None:
         if hessian:
             _save_hessian(name, th, build("serinv")[1])
             continue
+        if minimize:
+            _save_minimize(name, th, build("serinv")[1])
+            continue
         out = {"theta": th, "shape": np.array([ns, nt, nv, nb, no, seed])}
         for k, v in coreg_checksums(prob).items():
             out[f"chk_{k}"] = v
@@ -316,7 +319,10 @@ if __name__ == "__main__":
     _min = "--minimize" in sys.argv[2:]
     _only = [a for a in sys.argv[2:] if a not in ("--hessian", "--minimize")]
     if _min:
-        main(_root, [c for c in _only if c in CASES], minimize=True)
+        if any(c in CASES for c in _only):
+            main(_root, [c for c in _only if c in CASES], minimize=True)
+        if any(c in COREG_CASES for c in _only):
+            main_coregional(_root, [c for c in _only if c in COREG_CASES], minimize=True)
         sys.exit(0)
     if not _only or any(c in CASES for c in _only):
         main(_root, [c for c in _only if c in CASES], hessian=_hess)

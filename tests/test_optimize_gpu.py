@@ -43,3 +43,21 @@ def test_adjoint_driver_reaches_reference_optimum(name):
     # the adjoint gradient at the returned point is small, as L-BFGS-B's stop demands
     _, gr = model.objective_adjoint(r["theta"])
     assert np.max(np.abs(gr)) < 1.0
+
+
+def test_fd_driver_retraces_reference_coregional():
+    from golden_util import coreg_problem
+
+    from dalia_b200.coregional import CoregionalModel
+    from dalia_b200.optimize import minimize
+
+    g, ref = load("gst_coreg2_ragged"), load("min_gst_coreg2_ragged")
+    m = CoregionalModel(coreg_problem(g))
+    r = minimize(m, ref["theta0"], gradient="fd")
+    assert r["exit"] == "scipy" and r["success"]
+    assert len(r["f_values"]) == len(ref["f_values"])
+    np.testing.assert_allclose(r["f_values"], ref["f_values"], rtol=1e-8, atol=1e-8)
+    np.testing.assert_allclose(r["theta"], ref["theta"], rtol=1e-5, atol=1e-5)
+    # the adjoint driver reaches the same optimum
+    ra = minimize(CoregionalModel(coreg_problem(g)), ref["theta0"])
+    assert abs(ra["f"] - float(ref["f"])) < 1e-3 * max(1.0, abs(float(ref["f"])))

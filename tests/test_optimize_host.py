@@ -102,3 +102,31 @@ def test_no_hyperparameters_evaluates_once():
 def test_rejects_unknown_gradient():
     with pytest.raises(ValueError):
         minimize(Quadratic(), np.zeros(4), gradient="bfgs")
+
+
+class CoregOracleFD:
+    def __init__(self, prob):
+        from oracle.coreg_ref import CoregionalOracle
+
+        self.m = CoregionalOracle(prob)
+
+    def objective_fd(self, theta):
+        return self.m.objective(theta)
+
+    @property
+    def x(self):
+        return self.m.x
+
+
+def test_driver_reproduces_reference_minimize_coregional_prefix():
+    """The first three accepted iterates of the reference's run on the
+    2-variate coregional problem (the whole run takes a minute on the CPU;
+    the GPU test follows it to the end)."""
+    from golden_util import coreg_problem
+
+    g = load("gst_coreg2_ragged")
+    ref = load("min_gst_coreg2_ragged")
+    r = minimize(CoregOracleFD(coreg_problem(g)), ref["theta0"], gradient="fd", max_iter=3)
+    assert len(r["f_values"]) == 3
+    np.testing.assert_allclose(r["f_values"], ref["f_values"][:3], rtol=1e-9, atol=1e-9)
+    np.testing.assert_allclose(np.asarray(r["theta_values"]), ref["theta_values"][:3], rtol=1e-6, atol=1e-6)
