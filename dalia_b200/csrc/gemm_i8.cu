@@ -729,35 +729,48 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
     q.tmn = (p.M + QBM - 1) / QBM;
     q.tnn = (p.N + QBN - 1) / QBN;
     if ((p.cflags & GC_LOWER) && p.M != p.N) return cudaErrorInvalidValue;
-    int* eA = reinterpret_cast<int*>(w);
-    w += align256((size_t)p.M * 4);
-    int* fB = reinterpret_cast<int*>(w);
-    w += align256((size_t)p.N * 4);
-    q.eA = eA;
-    q.fB = fB;
     SliceGroup ga{}, gb{};
-    ga.exps = eA;
     ga.rows = p.M;
     ga.RB = 2 * q.tmn;
     ga.nseg = p.nseg;
-    gb.exps = fB;
     gb.rows = p.N;
     gb.RB = q.tnn;
     gb.nseg = p.nseg;
     for (int s = 0; s < p.nseg; ++s) {
       const GemmSeg& g = p.seg[s];
       const int KT = (g.K + QBK - 1) / QBK;
-      const int RBa = 2 * q.tmn, RBb = q.tnn;
-      int8_t* da = reinterpret_cast<int8_t*>(w);
-      w += align256((size_t)OZ_S * KT * RBa * IMG);
-      int8_t* db = reinterpret_cast<int8_t*>(w);
-      w += align256((size_t)OZ_S * KT * RBb * IMG);
-      ga.s[s] = SliceSeg{g.A, da, g.alpha, g.lda, g.K, (g.flags & GF_A_T) ? 0 : 1, KT};
-      gb.s[s] = SliceSeg{g.B, db, 1.0, g.ldb, g.K, (g.flags & GF_B_KN) ? 0 : 1, KT};
-      q.seg[s] = QSeg{da, db, KT, RBa, RBb, g.flags, g.K};
+      ga.s[s] = SliceSeg{g.A, nullptr, g.alpha, g.lda, g.K, (g.flags & GF_A_T) ? 0 : 1, KT};
+      gb.s[s] = SliceSeg{g.B, nullptr, 1.0, g.ldb, g.K, (g.flags & GF_B_KN) ? 0 : 1, KT};
     }
-    groups.push_back(ga);
-    groups.push_back(gb);
+    // a side equal to one already planned in this launch (same operands,
+    // orientation, scaling and image shape: e.g. the same block multiplied by
+    // the main and the arrow rows) shares its exponents and digit images;
+    // otherwise it gets its own
+    auto plan = [&](SliceGroup& gr) {
+      for (const SliceGroup& o : groups) {
+        bool eq = o.rows == gr.rows && o.RB == gr.RB && o.nseg == gr.nseg;
+        for (int s = 0; eq && s < gr.nseg; ++s)
+          eq = o.s[s].P == gr.s[s].P && o.s[s].alpha == gr.s[s].alpha && o.s[s].ld == gr.s[s].ld &&
+               o.s[s].K == gr.s[s].K && o.s[s].kcontig == gr.s[s].kcontig && o.s[s].KT == gr.s[s].KT;
+        if (eq) {
+          gr = o;
+          return;
+        }
+      }
+      gr.exps = reinterpret_cast<int*>(w);
+      w += align256((size_t)gr.rows * 4);
+      for (int s = 0; s < gr.nseg; ++s) {
+        gr.s[s].out = reinterpret_cast<int8_t*>(w);
+        w += align256((size_t)OZ_S * gr.s[s].KT * gr.RB * IMG);
+      }
+      groups.push_back(gr);
+    };
+    plan(ga);
+    plan(gb);
+    q.eA = ga.exps;
+    q.fB = gb.exps;
+    for (int s = 0; s < p.nseg; ++s)
+      q.seg[s] = QSeg{ga.s[s].out, gb.s[s].out, ga.s[s].KT, ga.RB, gb.RB, p.seg[s].flags, p.seg[s].K};
     qp.push_back(q);
   }
   // exponents and digits, SU image rows of a problem side per unit
