@@ -10,8 +10,9 @@
 // where every digit product sum is exact in INT32 (|a_p b_q| <= 127^2, at
 // most OZ_S pairs per d, K <= 19000).  Keeping the pairs with p + q <= OZ_S - 1
 // (28 of 49, digits counted from 0) drops products below 2^-7(OZ_S+2) 127^2
-// per element product: a relative error of ~1e-14 against sum_k |a||b| for
-// OZ_S = 7.  Seven digits are needed because the
+// per element product: an error of ~1e-14 relative to max_k |a_mk| max_k
+// |b_kn| K for OZ_S = 7 (small entries of a row or column with a wide range
+// keep fewer bits than their own magnitude would allow).  Seven digits are needed because the
 // selected inversion of an ill-conditioned precision (cond ~1e9 per block)
 // amplifies the truncation: five digits left gradient errors of 2e-3 at
 // b = 1500.
@@ -657,10 +658,14 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
           if (rw < P.M && col < P.N && (!lower || col <= rw)) {
             double* dst = C + (size_t)rw * P.ldc + col;
             double x = stage[rr * QSTAGE_LD + 32 * c + lane];
-            if (P.beta != 0.0) x += P.beta * *dst;
+            if (P.beta != 0.0) {
+              x += P.beta * *dst;
+              stage[rr * QSTAGE_LD + 32 * c + lane] = x;  // the mirror copies the final value
+            }
             *dst = x;
           }
         }
+        __syncwarp();
         // mirror: lane = row, so the transposed writes are contiguous too
         if (mirror && rowok) {
 #pragma unroll 4
