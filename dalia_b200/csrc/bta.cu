@@ -380,7 +380,8 @@ int bta_pobtas_batched(bta_handle_t h, int count, const int64_t* n, const int64_
         (a[k] > 0 && (!Ab || !T || !Ab[k] || !T[k])))
       return BTA_ERR_INVALID;
     const size_t nq = (b[k] + 63) / 64;
-    need += align_up(n[k] * nq * 4096 * 8) + align_up((n[k] * nq + 4) * 4) + 2 * kAlign;
+    need += align_up(n[k] * nq * 4096 * 8) + align_up((n[k] * nq + 4) * 4) + align_up((n[k] * a[k] + 1) * 8) +
+            3 * kAlign;
   }
   int rc = ensure_ws(h, need);
   if (rc) return rc;
@@ -416,9 +417,12 @@ int bta_pobtas_batched(bta_handle_t h, int count, const int64_t* n, const int64_
   }
   if (sweep_launch_batched(B, s)) return BTA_ERR_CUDA;
   if (trans == 0)
-    for (int k = 0; k < count; ++k)
-      if (arrow_forward(Ab ? Ab[k] : nullptr, T ? T[k] : nullptr, rhs[k], (int)n[k], (int)b[k], (int)a[k], s))
+    for (int k = 0; k < count; ++k) {
+      double* part = cv.take<double>((size_t)n[k] * a[k] + 1);
+      if (arrow_forward(Ab ? Ab[k] : nullptr, T ? T[k] : nullptr, rhs[k], (int)n[k], (int)b[k], (int)a[k], part,
+                        s))
         return BTA_ERR_CUDA;
+    }
   return cuda_rc(cudaGetLastError());
 }
 
@@ -621,7 +625,7 @@ int bta_pobtas_inv_batched(bta_handle_t h, int count, const int64_t* n, const in
     Lk[k] = n[k] > 1 ? L[k] : nullptr;
     Abk[k] = a[k] > 0 ? Ab[k] : nullptr;
     Tk[k] = a[k] > 0 ? T[k] : nullptr;
-    need += sweep_inv_work(bi[k]) * sizeof(double);
+    need += sweep_inv_work(ni[k], bi[k], ai[k]) * sizeof(double);
   }
   int rc = ensure_ws(h, align_up(need));
   if (rc) return rc;

@@ -33,13 +33,14 @@ struct SweepBatch {
 int diag_tile_inverses(const double* D, int n, int b, double* out, cudaStream_t s);
 int sweep_launch(const SweepArgs& A, cudaStream_t s);
 int sweep_launch_batched(SweepBatch& B, cudaStream_t s);
-int arrow_forward(const double* Ab, const double* T, double* x, int n, int b, int a, cudaStream_t s);
+// part: n * a doubles of scratch.
+int arrow_forward(const double* Ab, const double* T, double* x, int n, int b, int a, double* part, cudaStream_t s);
 int arrow_backward(const double* T, double* x, int n, int b, int a, cudaStream_t s);
 
 // Sweeps with precomputed block inverses V (solve_inv.cu): count instances,
-// x[k] of length n[k] b[k] + a[k]; work holds sweep_inv_work(b[k]) doubles
+// x[k] of length n[k] b[k] + a[k]; work holds sweep_inv_work(n[k], b[k], a[k]) doubles
 // per instance.
-size_t sweep_inv_work(int b);
+size_t sweep_inv_work(int n, int b, int a);
 int sweep_inv_batched(int count, const int* n, const int* b, const int* a, const double* const* L,
                       const double* const* Ab, const double* const* T, const double* const* V, double* const* x,
                       int trans, double* work, cudaStream_t s);

@@ -310,34 +310,59 @@ __global__ void __launch_bounds__(THREADS) sweep_kernel(const __grid_constant__ 
   }
 }
 
-// Forward arrow step: y_a = T^-1 (x_a - sum_i Ab_i y_i); one CTA.
-__global__ void __launch_bounds__(256) arrow_forward_kernel(const double* Ab, const double* Tt, double* x, int n,
-                                                            int b, int a) {
-  extern __shared__ double sa[];  // a values + 256 partials
-  double* ya = sa;
-  double* part = sa + a;
-  const int tid = threadIdx.x;
-  const long long nb = (long long)n * b;
-  for (int r = 0; r < a; ++r) {
-    double s = 0.0;
-    for (long long j = tid; j < nb; j += blockDim.x) {
-      const long long i = j / b, c = j % b;
-      s += Ab[(size_t)i * a * b + (size_t)r * b + c] * x[j];
+// Forward arrow step, y_a = T^-1 (x_a - sum_i Ab_i y_i), in two kernels:
+// one CTA per block i writes part[i a + r] = sum_c Ab_i[r][c] y_i[c] (its
+// arrow rows and y_i read once, AF_R rows at a time), then one CTA sums the
+// parts in block order (deterministic) and solves with the tip factor.
+constexpr int AF_THREADS = 256, AF_R = 8;
+
+__global__ void __launch_bounds__(AF_THREADS) arrow_part_kernel(const double* Ab, const double* x, int b, int a,
+                                                               double* part) {
+  __shared__ double red[AF_THREADS / 32][AF_R];
+  const int i = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double* xi = x + (size_t)i * b;
+  const double* Ai = Ab + (size_t)i * a * b;
+  for (int r0 = 0; r0 < a; r0 += AF_R) {
+    double acc[AF_R];
+#pragma unroll
+    for (int q = 0; q < AF_R; ++q) acc[q] = 0.0;
+    for (int c = tid; c < b; c += AF_THREADS) {
+      const double xv = xi[c];
+#pragma unroll
+      for (int q = 0; q < AF_R; ++q)
+        if (r0 + q < a) acc[q] = fma(Ai[(size_t)(r0 + q) * b + c], xv, acc[q]);
     }
-    part[tid] = s;
+#pragma unroll
+    for (int q = 0; q < AF_R; ++q)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < AF_R; ++q) red[warp][q] = acc[q];
     __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-      if (tid < o) part[tid] += part[tid + o];
-      __syncthreads();
+    if (tid < AF_R && r0 + tid < a) {
+      double sum = 0.0;
+      for (int w = 0; w < AF_THREADS / 32; ++w) sum += red[w][tid];
+      part[(size_t)i * a + r0 + tid] = sum;
     }
-    if (tid == 0) ya[r] = x[nb + r] - part[0];
     __syncthreads();
   }
-  if (tid == 0) {
+}
+
+__global__ void arrow_solve_kernel(const double* part, const double* Tt, double* x, int n, int b, int a) {
+  extern __shared__ double ya[];
+  const long long nb = (long long)n * b;
+  for (int r = threadIdx.x; r < a; r += blockDim.x) {
+    double sum = 0.0;
+    for (int i = 0; i < n; ++i) sum += part[(size_t)i * a + r];
+    ya[r] = x[nb + r] - sum;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
     for (int r = 0; r < a; ++r) {
-      double s = ya[r];
-      for (int k = 0; k < r; ++k) s -= Tt[r * a + k] * ya[k];
-      ya[r] = s / Tt[r * a + r];
+      double v = ya[r];
+      for (int k = 0; k < r; ++k) v -= Tt[r * a + k] * ya[k];
+      ya[r] = v / Tt[r * a + r];
       x[nb + r] = ya[r];
     }
   }
@@ -403,12 +428,16 @@ int sweep_launch(const SweepArgs& A, cudaStream_t s) {
   return sweep_launch_batched(B, s);
 }
 
-int arrow_forward(const double* Ab, const double* Tt, double* x, int n, int b, int a, cudaStream_t s) {
+int arrow_forward(const double* Ab, const double* Tt, double* x, int n, int b, int a, double* part,
+                  cudaStream_t s) {
   if (a <= 0) return cudaSuccess;
-  const size_t smem = (size_t)(a + 256) * sizeof(double);
   {
     bta::ProfScope _ps(bta::PROF_SWEEP, s);
-    arrow_forward_kernel<<<1, 256, smem, s>>>(Ab, Tt, x, n, b, a);
+    arrow_part_kernel<<<n, AF_THREADS, 0, s>>>(Ab, x, b, a, part);
+  }
+  {
+    bta::ProfScope _ps(bta::PROF_SWEEP, s);
+    arrow_solve_kernel<<<1, 128, (size_t)a * sizeof(double), s>>>(part, Tt, x, n, b, a);
   }
   return cudaGetLastError();
 }

@@ -176,18 +176,21 @@ int launch_cols(std::vector<ColJob>& jobs, cudaStream_t s) {
 
 }  // namespace
 
-size_t sweep_inv_work(int b) { return (size_t)b * (1 + (b + CT_ROWS - 1) / CT_ROWS); }
+size_t sweep_inv_work(int n, int b, int a) {
+  return (size_t)b * (1 + (b + CT_ROWS - 1) / CT_ROWS) + (size_t)n * a;
+}
 
 int sweep_inv_batched(int count, const int* n, const int* b, const int* a, const double* const* L,
                       const double* const* Ab, const double* const* T, const double* const* V, double* const* x,
                       int trans, double* work, cudaStream_t s) {
-  std::vector<double*> tmp(count), part(count);
+  std::vector<double*> tmp(count), part(count), apart(count);
   size_t off = 0;
   int maxn = 0;
   for (int k = 0; k < count; ++k) {
     tmp[k] = work + off;
     part[k] = work + off + b[k];
-    off += sweep_inv_work(b[k]);
+    apart[k] = work + off + (size_t)b[k] * (1 + (b[k] + CT_ROWS - 1) / CT_ROWS);
+    off += sweep_inv_work(n[k], b[k], a[k]);
     maxn = std::max(maxn, n[k]);
   }
   if (trans == 0) {
@@ -217,7 +220,7 @@ int sweep_inv_batched(int count, const int* n, const int* b, const int* a, const
       if (launch_rows(ja, s) || launch_rows(jb, s)) return cudaErrorUnknown;
     }
     for (int k = 0; k < count; ++k)
-      if (a[k] > 0 && arrow_forward(Ab[k], T[k], x[k], n[k], b[k], a[k], s)) return cudaErrorUnknown;
+      if (a[k] > 0 && arrow_forward(Ab[k], T[k], x[k], n[k], b[k], a[k], apart[k], s)) return cudaErrorUnknown;
     return cudaGetLastError();
   }
   for (int k = 0; k < count; ++k)
