@@ -64,6 +64,7 @@ SIGNATURES = {
     "bta_launch_count": (ctypes.c_longlong, []),
     "bta_pobtaf_noalloc": (_int, [_i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _pi64, _c_void_p]),
     "bta_noalloc_scratch_bytes": (ctypes.c_size_t, []),
+    "bta_noalloc_get_status": (_int, [_pi64, _c_void_p]),
     "bta_prof_enable": (_int, [_int]),
     "bta_prof_mask": (_int, [_int]),
     "bta_prof_read": (_int, [_pdbl, ctypes.POINTER(ctypes.c_longlong)]),

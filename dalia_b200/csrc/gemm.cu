@@ -199,12 +199,9 @@ __global__ void __launch_bounds__(THREADS) gemm_f64_kernel(const __grid_constant
 }  // namespace
 
 int gemm_launch(const std::vector<GemmProb>& probs, cudaStream_t stream) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(gemm_f64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)SMEM_BYTES);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
+  {
+    const int e = ensure_smem_attr(reinterpret_cast<const void*>(gemm_f64_kernel), (int)SMEM_BYTES);
+    if (e != cudaSuccess) return (cudaError_t)e;
   }
   size_t i = 0;
   while (i < probs.size()) {

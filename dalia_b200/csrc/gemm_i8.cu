@@ -711,12 +711,9 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
   if (ws_needed) *ws_needed = need;
   if (!ws) return cudaSuccess;
   if (ws_bytes < need || !abort_flag) return cudaErrorInvalidValue;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(gemm_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)QSMEM_BYTES);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
+  {
+    const int e = ensure_smem_attr(reinterpret_cast<const void*>(gemm_i8_kernel), (int)QSMEM_BYTES);
+    if (e != cudaSuccess) return (cudaError_t)e;
   }
   uint8_t* w = static_cast<uint8_t*>(ws);
   std::vector<SliceGroup> groups;
@@ -819,13 +816,7 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
     }
     b.tile_start[b.count] = total;
     if (total > 0) {
-      static int sms = 0;
-      if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        sms = std::max(1, sms);
-      }
+      const int sms = device_sm_count();
       bta::ProfScope _ps(bta::PROF_GEMM, stream);
       gemm_i8_kernel<<<std::min(total, sms), QTHREADS, QSMEM_BYTES, stream>>>(b, total, abort_flag);
     }

@@ -360,12 +360,9 @@ __global__ void __launch_bounds__(TTHREADS, 1) gemm_tc_kernel(const __grid_const
 }  // namespace
 
 int gemm_launch_tc(const std::vector<GemmProb>& probs, cudaStream_t stream, int* abort_flag) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e =
-        cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TSMEM_BYTES);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
+  {
+    const int e = ensure_smem_attr(reinterpret_cast<const void*>(gemm_tc_kernel), (int)TSMEM_BYTES);
+    if (e != cudaSuccess) return (cudaError_t)e;
   }
   if (!abort_flag) return cudaErrorInvalidValue;
   size_t i = 0;

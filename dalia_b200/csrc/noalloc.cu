@@ -9,7 +9,9 @@
 // of its scratch -- status words, launch task lists, inverses of the 64x64
 // diagonal tiles and per-tile dependency counters -- carved out of one
 // file-scope device array of fixed size (kScratchBytes, 2 MiB).  Every GPU
-// that loads this library holds that array until the process exits.
+// that loads this library holds that array until the process exits.  The
+// task lists are written by a small kernel, so a call reads no host memory
+// once it has returned.
 //
 // The array is shared by every call: it keeps the previous call's contents, so
 // each call clears what must start at zero, and calls whose work overlaps on
@@ -68,16 +70,29 @@ size_t panel_ws(int b, int a, bool hasL) {
   return align_up((size_t)nq * 4096 * sizeof(double)) + align_up(((size_t)2 * nr * nq + 4) * sizeof(int));
 }
 
-std::vector<int4> tasks_for(int b, int a, bool hasL) {
-  bta::PanelInst I{};
-  I.b = b;
-  I.a = a;
-  I.nq = (b + 63) / 64;
-  I.L = hasL ? reinterpret_cast<double*>(1) : nullptr;
-  I.nrows_t = bta::panel_rows(b, a, hasL);
-  std::vector<int4> t;
-  bta::panel_tasks({I}, t);
-  return t;
+// Task list of one panel with no previous-column or tip tasks (the shape this
+// entry point launches): tile column r holds nr - r tasks, the diagonal tile
+// (r, r) first, then tiles p = r+1 .. nr-1 in order -- the tile just below
+// the diagonal tile (p = r+1 < nq) is handed to the chain CTA, every other
+// tile gets its triangular solve.  This is the order bta::panel_tasks
+// produces for such a panel (checked on the CPU against bta_panel_task_list).
+int task_count(int nq, int nr) { return nq * nr - nq * (nq - 1) / 2; }
+
+__global__ void write_tasks_kernel(int4* out, int nq, int nr) {
+  const int r = blockIdx.x;
+  if (r >= nq) return;
+  const int off = r * nr - r * (r - 1) / 2;
+  for (int j = threadIdx.x; j < nr - r; j += blockDim.x) {
+    const int p = r + j;
+    const int kind = j == 0 ? bta::TASK_AGG_DIAG : (p == r + 1 && p < nq ? bta::TASK_AGG_SUB : bta::TASK_AGG_TRSM);
+    out[off + j] = make_int4(0, kind, p, r);
+  }
+}
+
+int write_tasks(int4* out, int b, int a, bool hasL, cudaStream_t s) {
+  const int nq = (b + 63) / 64, nr = bta::panel_rows(b, a, hasL);
+  write_tasks_kernel<<<nq, 128, 0, s>>>(out, nq, nr);
+  return cudaGetLastError() == cudaSuccess ? BTA_OK : BTA_ERR_CUDA;
 }
 
 // Status words: [0] abort flag (int), [8] first failing pivot (u64).
@@ -123,38 +138,34 @@ size_t bta_noalloc_scratch_bytes(void) { return kScratchBytes; }
 int bta_pobtaf_noalloc(int64_t n, int64_t b, int64_t a, double* D, double* L, double* Ab, double* T, int64_t* info,
                        void* stream) {
   if (n < 1 || b < 1 || a < 0 || !D || (n > 1 && !L) || (a > 0 && (!Ab || !T))) return BTA_ERR_INVALID;
-  if (b > 65535 || a > 4096) return BTA_ERR_INVALID;
+  if (b > BTA_NOALLOC_MAX_B || a > BTA_NOALLOC_MAX_A) return BTA_ERR_INVALID;
   cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-  const std::vector<int4> tL = n > 1 ? tasks_for((int)b, (int)a, true) : std::vector<int4>();
-  const std::vector<int4> t0 = tasks_for((int)b, (int)a, false);
-  const std::vector<int4> tT = a > 0 ? tasks_for((int)a, 0, false) : std::vector<int4>();
+  const int B_ = (int)b, A_ = (int)a;
+  const int nqb = (B_ + 63) / 64, nqa = (A_ + 63) / 64;
+  const int nL = n > 1 ? task_count(nqb, bta::panel_rows(B_, A_, true)) : 0;
+  const int n0 = task_count(nqb, bta::panel_rows(B_, A_, false));
+  const int nT = a > 0 ? task_count(nqa, bta::panel_rows(A_, 0, false)) : 0;
   Layout lay;
-  lay.ws_bytes = std::max(panel_ws((int)b, (int)a, true), a > 0 ? panel_ws((int)a, 0, false) : size_t(0));
+  lay.ws_bytes = std::max(panel_ws(B_, A_, true), a > 0 ? panel_ws(A_, 0, false) : size_t(0));
   lay.off_ws = kAlign;
   lay.off_tasksL = lay.off_ws + align_up(lay.ws_bytes);
-  lay.off_tasks0 = lay.off_tasksL + align_up(tL.size() * sizeof(int4));
-  lay.off_tasksT = lay.off_tasks0 + align_up(t0.size() * sizeof(int4));
-  lay.total = lay.off_tasksT + align_up(tT.size() * sizeof(int4));
-  if (lay.total > kScratchBytes) return BTA_ERR_INVALID;  // block too large for the fixed scratch
+  lay.off_tasks0 = lay.off_tasksL + align_up((size_t)nL * sizeof(int4));
+  lay.off_tasksT = lay.off_tasks0 + align_up((size_t)n0 * sizeof(int4));
+  lay.total = lay.off_tasksT + align_up((size_t)nT * sizeof(int4));
+  if (lay.total > kScratchBytes) return BTA_ERR_INVALID;  // cannot happen within the limits above
 
   char* base = nullptr;
   int rc = scratch_address(&base);
   if (rc) return rc;
-  // clear the status words; upload this call's task lists
+  // clear the status words; write this call's task lists
   if (cudaMemsetAsync(base, 0, 8, s) != cudaSuccess) return BTA_ERR_CUDA;
   if (cudaMemsetAsync(base + 8, 0xff, 8, s) != cudaSuccess) return BTA_ERR_CUDA;
-  const int4* dL = reinterpret_cast<const int4*>(base + lay.off_tasksL);
-  const int4* d0 = reinterpret_cast<const int4*>(base + lay.off_tasks0);
-  const int4* dT = reinterpret_cast<const int4*>(base + lay.off_tasksT);
-  if (!tL.empty() && cudaMemcpyAsync(base + lay.off_tasksL, tL.data(), tL.size() * sizeof(int4),
-                                     cudaMemcpyHostToDevice, s) != cudaSuccess)
-    return BTA_ERR_CUDA;
-  if (!t0.empty() && cudaMemcpyAsync(base + lay.off_tasks0, t0.data(), t0.size() * sizeof(int4),
-                                     cudaMemcpyHostToDevice, s) != cudaSuccess)
-    return BTA_ERR_CUDA;
-  if (!tT.empty() && cudaMemcpyAsync(base + lay.off_tasksT, tT.data(), tT.size() * sizeof(int4),
-                                     cudaMemcpyHostToDevice, s) != cudaSuccess)
-    return BTA_ERR_CUDA;
+  int4* dL = reinterpret_cast<int4*>(base + lay.off_tasksL);
+  int4* d0 = reinterpret_cast<int4*>(base + lay.off_tasks0);
+  int4* dT = reinterpret_cast<int4*>(base + lay.off_tasksT);
+  if (nL > 0 && (rc = write_tasks(dL, B_, A_, true, s))) return rc;
+  if ((rc = write_tasks(d0, B_, A_, false, s))) return rc;
+  if (nT > 0 && (rc = write_tasks(dT, A_, 0, false, s))) return rc;
 
   const size_t bb = (size_t)b * b, ab = (size_t)a * b;
   for (int64_t i = 0; i < n; ++i) {
@@ -162,44 +173,48 @@ int bta_pobtaf_noalloc(int64_t n, int64_t b, int64_t a, double* D, double* L, do
     double* Di = D + i * bb;
     double* Li = hasL ? L + i * bb : nullptr;
     double* Abi = a > 0 ? Ab + i * ab : nullptr;
-    rc = run_panel(base, lay, hasL ? dL : d0, hasL ? (int)tL.size() : (int)t0.size(), Di, Li, Abi, (int)b, (int)a,
-                   (long long)(i * b), s);
+    rc = run_panel(base, lay, hasL ? dL : d0, hasL ? nL : n0, Di, Li, Abi, B_, A_, (long long)(i * b), s);
     if (rc) return rc;
     std::vector<bta::GemmProb> probs;
     if (hasL) {
-      bta::GemmProb p = bta::gemm_prob(D + (i + 1) * bb, (int)b, (int)b, (int)b, 1.0, bta::GC_LOWER);
-      bta::gemm_add(p, Li, (int)b, Li, (int)b, (int)b, -1.0, 0);
+      bta::GemmProb p = bta::gemm_prob(D + (i + 1) * bb, B_, B_, B_, 1.0, bta::GC_LOWER);
+      bta::gemm_add(p, Li, B_, Li, B_, B_, -1.0, 0);
       probs.push_back(p);
     }
     if (a > 0) {
       if (hasL) {
-        bta::GemmProb p = bta::gemm_prob(Ab + (i + 1) * ab, (int)b, (int)a, (int)b, 1.0);
-        bta::gemm_add(p, Abi, (int)b, Li, (int)b, (int)b, -1.0, 0);
+        bta::GemmProb p = bta::gemm_prob(Ab + (i + 1) * ab, B_, A_, B_, 1.0);
+        bta::gemm_add(p, Abi, B_, Li, B_, B_, -1.0, 0);
         probs.push_back(p);
       }
-      bta::GemmProb p = bta::gemm_prob(T, (int)a, (int)a, (int)a, 1.0);
-      bta::gemm_add(p, Abi, (int)b, Abi, (int)b, (int)b, -1.0, 0);
+      bta::GemmProb p = bta::gemm_prob(T, A_, A_, A_, 1.0);
+      bta::gemm_add(p, Abi, B_, Abi, B_, B_, -1.0, 0);
       probs.push_back(p);
     }
     if (!probs.empty() && bta::gemm_launch(probs, s) != cudaSuccess) return BTA_ERR_CUDA;
   }
   if (a > 0) {
-    rc = run_panel(base, lay, dT, (int)tT.size(), T, nullptr, nullptr, (int)a, 0, (long long)(n * b), s);
+    rc = run_panel(base, lay, dT, nT, T, nullptr, nullptr, A_, 0, (long long)(n * b), s);
     if (rc) return rc;
   }
   if (cudaGetLastError() != cudaSuccess) return BTA_ERR_CUDA;
-  if (info) {
-    unsigned long long hinfo = 0;
-    int habort = 0;
-    if (cudaStreamSynchronize(s) != cudaSuccess) return BTA_ERR_CUDA;
-    if (cudaMemcpy(&habort, base, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return BTA_ERR_CUDA;
-    if (cudaMemcpy(&hinfo, base + 8, sizeof(hinfo), cudaMemcpyDeviceToHost) != cudaSuccess) return BTA_ERR_CUDA;
-    const bool fail = hinfo != ~0ULL;
-    *info = fail ? (int64_t)hinfo : 0;
-    if (habort) return BTA_ERR_TIMEOUT;
-    if (fail) return BTA_ERR_NOT_SPD;
-  }
+  if (info) return bta_noalloc_get_status(info, stream);
   return BTA_OK;
+}
+
+int bta_noalloc_get_status(int64_t* info, void* stream) {
+  char* base = nullptr;
+  int rc = scratch_address(&base);
+  if (rc) return rc;
+  unsigned long long hinfo = 0;
+  int habort = 0;
+  if (cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess) return BTA_ERR_CUDA;
+  if (cudaMemcpy(&habort, base, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return BTA_ERR_CUDA;
+  if (cudaMemcpy(&hinfo, base + 8, sizeof(hinfo), cudaMemcpyDeviceToHost) != cudaSuccess) return BTA_ERR_CUDA;
+  const bool fail = hinfo != ~0ULL;
+  if (info) *info = fail ? (int64_t)hinfo : 0;
+  if (habort) return BTA_ERR_TIMEOUT;
+  return fail ? BTA_ERR_NOT_SPD : BTA_OK;
 }
 
 }  // extern "C"

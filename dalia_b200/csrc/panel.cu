@@ -551,18 +551,13 @@ void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks) 
 }
 
 int panel_grid_size() {
-  static int grid = 0;
-  if (grid == 0) {
-    cudaError_t e = cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)SMEM_BYTES);
-    if (e != cudaSuccess) return -(int)e;
-    int dev = 0, sms = 0, occ = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel, THREADS, SMEM_BYTES);
-    grid = std::max(2, sms * std::max(1, occ));
-  }
-  return grid;
+  const int e = ensure_smem_attr(reinterpret_cast<const void*>(panel_kernel), (int)SMEM_BYTES);
+  if (e != cudaSuccess) return -e;
+  // one resident CTA per SM at this shared-memory size (the occupancy query
+  // is cheap next to a panel launch, and answers for the current device)
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel, THREADS, SMEM_BYTES);
+  return std::max(2, device_sm_count() * std::max(1, occ));
 }
 
 int panel_launch(const PanelBatch& batch, int grid, cudaStream_t stream) {

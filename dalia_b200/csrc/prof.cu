@@ -1,6 +1,9 @@
 // Launch counter and optional per-category CUDA-event timing (prof.cuh).
 #include <atomic>
+#include <map>
 #include <mutex>
+#include <set>
+#include <tuple>
 #include <vector>
 
 #include "../../include/dalia_bta.h"
@@ -34,7 +37,37 @@ cudaEvent_t take_event() {
   return e;
 }
 
+std::mutex g_attr_mu;
+std::set<std::tuple<const void*, int, int>> g_attr_done;  // (kernel, device, bytes)
+std::map<int, int> g_sms;
+
 }  // namespace
+
+int ensure_smem_attr(const void* kernel, int bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  const auto key = std::make_tuple(kernel, dev, bytes);
+  if (g_attr_done.count(key)) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  g_attr_done.insert(key);
+  return cudaSuccess;
+}
+
+int device_sm_count() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+  std::lock_guard<std::mutex> lk(g_attr_mu);
+  auto it = g_sms.find(dev);
+  if (it == g_sms.end()) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    it = g_sms.emplace(dev, sms).first;
+  }
+  return it->second;
+}
 
 void prof_begin(int cat, cudaStream_t s, cudaEvent_t* ev) {
   g_launches.fetch_add(1, std::memory_order_relaxed);

@@ -21,6 +21,16 @@ enum ProfCat : int {
 void prof_begin(int cat, cudaStream_t s, cudaEvent_t* ev);
 void prof_end(int cat, cudaStream_t s, cudaEvent_t ev);
 
+// Per-device launch set-up.  A kernel attribute such as its dynamic
+// shared-memory limit belongs to the kernel on one device, so the helpers
+// below remember what they did per (kernel, device), under a mutex: a process
+// may drive several GPUs from several host threads.
+// ensure_smem_attr: raise the kernel's dynamic shared-memory limit on the
+// current device (once per device); returns a cudaError_t.
+int ensure_smem_attr(const void* kernel, int bytes);
+// Number of SMs of the current device (cached per device).
+int device_sm_count();
+
 struct ProfScope {
   int cat;
   cudaStream_t s;

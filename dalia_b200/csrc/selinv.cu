@@ -210,12 +210,9 @@ __global__ void logdet_final_kernel(const double* part, int cnt, double* out) {
 }  // namespace
 
 int block_trtri(const double* D, const double* tile_inv, int i0, int i1, int b, double* out, cudaStream_t s) {
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e =
-        cudaFuncSetAttribute(block_trtri_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRTRI_SMEM);
+  {
+    const int e = ensure_smem_attr(reinterpret_cast<const void*>(block_trtri_kernel), (int)TRTRI_SMEM);
     if (e != cudaSuccess) return e;
-    attr = true;
   }
   const int nblk = i1 - i0, nq = (b + T - 1) / T;
   if (nblk <= 0) return cudaSuccess;

@@ -383,12 +383,9 @@ __global__ void arrow_backward_kernel(const double* Tt, double* x, long long nb,
 int diag_tile_inverses(const double* D, int n, int b, double* out, cudaStream_t s) {
   const int nq = (b + T - 1) / T;
   const size_t smem = size_t(2) * T * SG * sizeof(double);
-  static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(diag_tile_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+  {
+    const int e = ensure_smem_attr(reinterpret_cast<const void*>(diag_tile_inverse_kernel), (int)smem);
     if (e != cudaSuccess) return e;
-    attr = true;
   }
   if (n * nq == 0) return cudaSuccess;
   {
@@ -403,13 +400,10 @@ int sweep_launch_batched(SweepBatch& B, cudaStream_t s) {
   for (int k = 0; k < B.count; ++k) maxt = std::max(maxt, B.inst[k].n * B.inst[k].nq);
   B.total = B.count * maxt;
   if (B.total == 0) return cudaSuccess;
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * T * SP * sizeof(double)));
-    attr = true;
+  const int sms = device_sm_count();
+  {
+    const int e = ensure_smem_attr(reinterpret_cast<const void*>(sweep_kernel), (int)(2 * T * SP * sizeof(double)));
+    if (e != cudaSuccess) return e;
   }
   const int grid = std::min(B.total, sms * 3);
   {

@@ -191,20 +191,27 @@ int bta_gather_coo(bta_handle_t h, int64_t n, int64_t b, int64_t a, const int64_
  * it exists for callers that may not call cudaMalloc/cudaFree themselves or
  * through a library -- code inside a framework whose pool allocator owns the
  * GPU's memory, or latency-critical loops that cannot afford cudaFree's
- * device-wide synchronisation.  Same arguments and results as bta_pobtaf
- * (including info), but no handle: the work runs on `stream` (a
- * cudaStream_t, NULL = legacy default stream) and all scratch lives in one
- * fixed 2 MiB device array inside the library (bta_noalloc_scratch_bytes),
- * which every GPU that loads the library holds until the process exits.
- * That is enough for diagonal blocks up to b = 2048 with an arrowhead of up to
- * 64 rows; larger problems are rejected with BTA_ERR_INVALID before any GPU
- * work.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) -- make that first call before any stream capture.
+ * device-wide synchronisation.  Same arguments and results as bta_pobtaf, but
+ * no handle: the work runs on `stream` (a cudaStream_t, NULL = legacy default
+ * stream) and all scratch lives in one fixed 2 MiB device array inside the
+ * library (bta_noalloc_scratch_bytes), which every GPU that loads the library
+ * holds until the process exits.  Sizes: b <= BTA_NOALLOC_MAX_B and
+ * a <= BTA_NOALLOC_MAX_A (any n); larger problems are rejected with
+ * BTA_ERR_INVALID before any GPU work.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) -- make that first call
+ * before any stream capture.  With info != NULL the call synchronises the
+ * stream and reports a non-positive pivot (info, BTA_ERR_NOT_SPD) or a
+ * timed-out device wait (BTA_ERR_TIMEOUT).  With info == NULL it returns
+ * without waiting; the status stays in the array until the next call clears
+ * it, and bta_noalloc_get_status (same stream) synchronises and reads it.
  * All calls share the array and each clears what must start at zero, so calls
  * whose work overlaps on the GPU (other streams, other threads) race.
  */
+#define BTA_NOALLOC_MAX_B 2048
+#define BTA_NOALLOC_MAX_A 128
 int bta_pobtaf_noalloc(int64_t n, int64_t b, int64_t a, double* D, double* L, double* Ab, double* T, int64_t* info,
                        void* stream);
+int bta_noalloc_get_status(int64_t* info, void* stream);
 size_t bta_noalloc_scratch_bytes(void);
 
 /*

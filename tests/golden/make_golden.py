@@ -314,7 +314,10 @@ if __name__ == "__main__":
     # usage: make_golden.py [REF_ROOT [--hessian | --minimize] [CASE ...]]
     #   --hessian writes hess_<CASE>.npz (the reference's FD Hessian) instead,
     #   --minimize writes min_<CASE>.npz (the reference's DALIA.minimize)
-    _root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DALIA_REF", "/root/reference")
+    _root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DALIA_REF")
+    if not _root or not os.path.isdir(os.path.join(_root, "src", "dalia")):
+        sys.exit("usage: make_golden.py REF_ROOT [--hessian | --minimize] [CASE ...]  (or set DALIA_REF): "
+                 "REF_ROOT is a DALIA checkout containing src/dalia")
     _hess = "--hessian" in sys.argv[2:]
     _min = "--minimize" in sys.argv[2:]
     _only = [a for a in sys.argv[2:] if a not in ("--hessian", "--minimize")]

@@ -208,3 +208,25 @@ def test_task_list_rejects_bad_arguments():
     zero = (ctypes.c_int * 1)(0)
     assert lib.bta_panel_task_list(0, one, zero, zero, None, 0, ctypes.byref(n)) == _lib.BTA_ERR_INVALID
     assert lib.bta_panel_task_list(1, zero, zero, zero, None, 0, ctypes.byref(n)) == _lib.BTA_ERR_INVALID
+
+
+def noalloc_order(b, a, has_l):
+    """The closed form the allocation-free factorisation writes on the device
+    (``write_tasks_kernel`` in ``noalloc.cu``): tile column r holds the
+    diagonal tile, then tiles r+1 .. rows-1 in order, the tile right below the
+    diagonal tile going to the chain CTA."""
+    inst = Inst(b, a, HAS_L if has_l else 0)
+    out = []
+    for r in range(inst.nq):
+        out.append((0, DIAG, r, r))
+        for p in range(r + 1, inst.rows):
+            out.append((0, SUB if (p == r + 1 and p < inst.nq) else TRSM, p, r))
+    assert len(out) == inst.nq * inst.rows - inst.nq * (inst.nq - 1) // 2
+    return out
+
+
+@pytest.mark.parametrize("b", [1, 63, 64, 65, 200, 1500, 2048])
+@pytest.mark.parametrize("a", [0, 5, 64, 100, 128])
+@pytest.mark.parametrize("has_l", [False, True])
+def test_noalloc_device_task_order_matches_queue(b, a, has_l):
+    assert task_list([Inst(b, a, HAS_L if has_l else 0)]) == noalloc_order(b, a, has_l)
