@@ -3,22 +3,27 @@ spatio-temporal INLA workload (default: Gaussian DEMF(1,2,1), ns = 1500,
 nt = 100, nb = 6, 600 observations per step; BTA blocks 1500 x 1500).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME] [--batch K] [--precision fp64|i8slice|tf32x3]
 
 One step = full gradient evaluations (f(theta) and grad f) at ``--batch``
 theta points (the candidates of a line search, default 3), the unit counted
 being one gradient evaluation.  ``ours`` uses the adjoint path (one
 factorisation and selected inversion of Q_c and of Q_prior per point, all 2K
 matrices factored and inverted together); the single-point adjoint and the
-plain FP64 central-difference path (2d+1 evaluations of f, one after another,
-as the reference computes it) are timed beside it.
+plain FP64 central-difference paths (2d+1 evaluations of f, one after
+another as the reference computes them, and the same stencil with its points
+factorised together) are timed beside it, warm, over ``--fd-steps`` repeats.
+A mixed-size workload (``synth.MIXED_BATCHES``) evaluates the points of
+several models -- instances of different block sizes -- in shared launches.
 With N > 1 (torchrun) every rank evaluates its own replica (independent theta
 points, no collective on the data path); the reported value is the total over
 ranks divided by the slowest rank's device time.
 
 ``--impl reference`` times the CPU oracle (NumPy/SciPy LAPACK restatement of
-the reference's Serinv path) on the host cores on a bounded sample: one f(theta)
-on the workload truncated to ``--cpu-nt`` time steps, scaled to the full
-workload and to the 2d+1 evaluations of a finite-difference gradient.
+the reference's Serinv path) on the host cores: every step is one f(theta) on
+the workload truncated to ``--cpu-nt`` time steps, scaled to the full workload
+and to the 2d+1 evaluations of a finite-difference gradient; one f(theta) on
+the whole workload (``--ref-full-nt``) checks that linear scaling in nt.
 """
 
 from __future__ import annotations
@@ -41,7 +46,7 @@ sys.path.insert(0, REPO)
 METRIC = "grad log pi(theta|y) evals/s"
 
 
-def parse():
+def parse(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
@@ -49,13 +54,18 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="gst_1500x100")
     p.add_argument("--cpu-nt", type=int, default=10)
-    p.add_argument("--fd-steps", type=int, default=1)
+    p.add_argument("--ref-full-nt", type=int, default=1,
+                   help="reference arm: also time one f(theta) on the untruncated workload (0: skip)")
+    p.add_argument("--fd-steps", type=int, default=3, help="timed repeats of each FD path (after one warm-up)")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-oracle baseline sample")
     p.add_argument("--batch", type=int, default=3,
-                   help="theta points per step (a line-search batch), factorised together")
+                   help="theta points per step (a line-search batch), factorised together; "
+                        "reduced to what device memory holds")
     p.add_argument("--precision", default="i8slice", choices=["fp64", "tf32x3", "i8slice"],
                    help="arithmetic of the selected inversions behind the adjoint gradient")
-    return p.parse_args()
+    p.add_argument("--factor-precision", default="fp64", choices=["fp64", "i8slice"],
+                   help="arithmetic of the factorisations' previous-column Schur updates in the adjoint path")
+    return p.parse_args(argv)
 
 
 def dist_info():
@@ -93,34 +103,92 @@ def job_rate(units_per_rank, world, t_max):
     return units_per_rank * world / t_max
 
 
+# ------------------------------------------------------------- workloads
+def members(workload):
+    """[(single workload, theta points per step or None)] of a workload: one
+    member for a plain workload, several for a mixed-size batch."""
+    from dalia_b200 import synth
+
+    if workload in synth.MIXED_BATCHES:
+        return list(synth.MIXED_BATCHES[workload])
+    if workload in synth.CONFIGS or workload in synth.COREG_CONFIGS:
+        return [(workload, None)]
+    raise SystemExit(f"unknown workload {workload!r}")
+
+
+def config_of(name):
+    from dalia_b200 import synth
+
+    return synth.COREG_CONFIGS[name] if name in synth.COREG_CONFIGS else synth.CONFIGS[name]
+
+
 # ----------------------------------------------------------------- CPU port
 def cpu_sample(workload, nt_sample, reps=1):
     """Time one f(theta) of the CPU oracle on the workload truncated to
-    nt_sample time steps; returns (seconds per full FD gradient, description)."""
+    nt_sample time steps; returns (seconds per full FD gradient, description,
+    seconds of the sampled f).  A mixed-size batch is timed member by member
+    and weighted by its points per step (seconds per gradient, averaged)."""
     from dalia_b200 import synth
     from oracle import coreg_ref, model_ref
 
-    coreg = workload in synth.COREG_CONFIGS
-    cfg = dict(synth.COREG_CONFIGS[workload] if coreg else synth.CONFIGS[workload])
-    nt_full = cfg["nt"]
-    cfg["nt"] = min(nt_sample, nt_full)
-    if coreg:
-        om = coreg_ref.CoregionalOracle(synth.make_coregional_problem(seed=0, **cfg))
-    else:
-        om = model_ref.OracleModel(synth.make_problem(seed=0, **cfg))
+    mem = members(workload)
+    total_pts = sum(k or 1 for _, k in mem)
+    t_grad, descs, t_sample = 0.0, [], 0.0
+    for name, k in mem:
+        coreg = name in synth.COREG_CONFIGS
+        cfg = dict(config_of(name))
+        nt_full = cfg["nt"]
+        cfg["nt"] = min(nt_sample, nt_full)
+        if coreg:
+            om = coreg_ref.CoregionalOracle(synth.make_coregional_problem(seed=0, **cfg))
+        else:
+            om = model_ref.OracleModel(synth.make_problem(seed=0, **cfg))
+        th = np.asarray(cfg["theta"], dtype=np.float64)
+        om.evaluate_f(th)  # warm-up (BLAS thread pool, caches)
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            om.evaluate_f(th)
+            ts.append(time.perf_counter() - t0)
+        t_sample += min(ts)
+        t_f = min(ts) * nt_full / cfg["nt"]
+        d = th.size
+        t_grad += (k or 1) / total_pts * t_f * (2 * d + 1)
+        descs.append(f"{name}: one f(theta) truncated to nt={cfg['nt']} of {nt_full}, scaled linearly in nt "
+                     f"and by 2d+1={2 * d + 1} evaluations per FD gradient")
+    desc = "CPU oracle (NumPy/SciPy LAPACK): " + "; ".join(descs)
+    return t_grad, desc, t_sample
+
+
+def full_nt_check(workload, max_s=150.0):
+    """One f(theta) of the CPU oracle on the untruncated (first) member of the
+    workload, against the linear extrapolation from a 10-step sample; skipped
+    when the extrapolation says it would take longer than max_s."""
+    from dalia_b200 import synth
+    from oracle import coreg_ref, model_ref
+
+    name = members(workload)[0][0]
+    cfg = dict(config_of(name))
+    make = (lambda c: coreg_ref.CoregionalOracle(synth.make_coregional_problem(seed=0, **c))) \
+        if name in synth.COREG_CONFIGS else (lambda c: model_ref.OracleModel(synth.make_problem(seed=0, **c)))
     th = np.asarray(cfg["theta"], dtype=np.float64)
-    om.evaluate_f(th)  # warm-up (BLAS thread pool, caches)
-    ts = []
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        om.evaluate_f(th)
-        ts.append(time.perf_counter() - t0)
-    t_f = min(ts) * nt_full / cfg["nt"]
-    d = th.size
-    t_grad = t_f * (2 * d + 1)
-    desc = (f"one f(theta) of the CPU oracle (NumPy/SciPy LAPACK) on {workload} truncated to nt={cfg['nt']} "
-            f"of {nt_full}, scaled linearly in nt and by 2d+1={2 * d + 1} evaluations per FD gradient")
-    return t_grad, desc
+    small = dict(cfg, nt=min(10, cfg["nt"]))
+    os_ = make(small)
+    os_.evaluate_f(th)
+    t0 = time.perf_counter()
+    os_.evaluate_f(th)
+    t_small = time.perf_counter() - t0
+    extrap = t_small * cfg["nt"] / small["nt"]
+    out = {"workload": name, "nt": cfg["nt"], "f_nt10_s": t_small, "extrapolated_full_s": extrap}
+    if extrap > max_s:
+        out["skipped"] = f"extrapolated {extrap:.0f} s > {max_s:.0f} s"
+        return out
+    om = make(cfg)
+    t0 = time.perf_counter()
+    om.evaluate_f(th)
+    t_full = time.perf_counter() - t0
+    out.update({"f_full_nt_s": t_full, "measured_over_extrapolated": t_full / extrap})
+    return out
 
 
 def run_reference(args):
@@ -131,11 +199,17 @@ def run_reference(args):
     ts = []
     desc = ""
     for i in range(args.warmup + args.steps):
-        t, desc = cpu_sample(args.workload, args.cpu_nt)
+        t, desc, _ = cpu_sample(args.workload, args.cpu_nt)
         if i >= args.warmup:
             ts.append(t)
     t_step = statistics.median(ts)
     value = 1.0 / t_step
+    check = None
+    if getattr(args, "ref_full_nt", 0):
+        try:
+            check = full_nt_check(args.workload)
+        except MemoryError as exc:  # config 4 needs ~64 GB of host memory per matrix
+            check = {"skipped": repr(exc)}
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -153,6 +227,7 @@ def run_reference(args):
         "config": {"workload": args.workload, "path": "central finite differences, FP64, CPU oracle"},
         "cpu_baseline": {"value": value, "unit": "evals/s", "cores": cores, "kind": "port", "sample": desc},
         "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "nt_scaling_check": check,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -222,12 +297,47 @@ def measured_fp64_peak(torch, dev):
     return 2.0 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
+def panel_bytes_per_launch(b, a, count):
+    """Algorithmic DRAM bytes of one block-column launch of the factorisation
+    over count matrices: D_i, L_i and Ab_i read and written once, the previous
+    column's L_{i-1} and Ab_{i-1} read once."""
+    return count * 8 * (2 * (2 * b * b + a * b) + b * b + a * b)
+
+
+def roofline_traffic(workload, kernel, shape):
+    """DRAM bytes per launch of the dominant kernel: the ncu capture of the
+    same launch shape if one is committed, else the capture of the nearest
+    shape scaled by the algorithmic bytes per launch (said in the source)."""
+    path = os.path.join(REPO, "profiles", "traffic.json")
+    try:
+        tab = json.load(open(path))
+    except Exception:
+        return None, "no capture"
+    caps = tab.get("captures", {})
+    b, a, count = shape
+    for key, cap in caps.items():
+        if kernel in cap and tuple(cap.get("shape", ())) == (b, a, count):
+            return float(cap[kernel]), f"ncu capture {key} (same launch shape)"
+    for key, cap in caps.items():
+        if kernel in cap and "shape" in cap:
+            cb, ca, cc = cap["shape"]
+            if kernel == "panel":
+                scale = panel_bytes_per_launch(b, a, count) / panel_bytes_per_launch(cb, ca, cc)
+            else:
+                scale = (b * b * count) / (cb * cb * cc)
+            return float(cap[kernel]) * scale, (f"ncu capture {key} (launch shape b={cb}, a={ca}, {cc} matrices) "
+                                                f"scaled by algorithmic bytes per launch x{scale:.3f}")
+    return None, "no capture"
+
+
 def run_ours(args):
+    import ctypes
+
     import torch
 
     from dalia_b200 import _lib, synth
     from dalia_b200.coregional import CoregionalModel
-    from dalia_b200.model import SpatioTemporalModel
+    from dalia_b200.model import SpatioTemporalModel, adjoint_group
 
     rank, world, local = dist_info()
     if world > 1:
@@ -237,13 +347,25 @@ def run_ours(args):
     dev = torch.device("cuda", torch.cuda.current_device())
     lib = _lib.load()
 
-    coreg = args.workload in synth.COREG_CONFIGS
-    cfg = synth.COREG_CONFIGS[args.workload] if coreg else synth.CONFIGS[args.workload]
-    prob = synth.make_config(args.workload, seed=0)
-    model = (CoregionalModel if coreg else SpatioTemporalModel)(prob, device=dev, selinv_precision=args.precision)
-    n, b, a = model.nt, model.b, model.nb
-    # replicas evaluate different theta points (a line-search batch)
-    theta = replica_theta(cfg["theta"], rank)
+    mem = members(args.workload)
+    models, thetas, Ks = [], [], []
+    for name, k in mem:
+        prob = synth.make_config(name, seed=0)
+        cls = CoregionalModel if name in synth.COREG_CONFIGS else SpatioTemporalModel
+        m = cls(prob, device=dev, selinv_precision=args.precision, factor_precision=args.factor_precision)
+        models.append(m)
+        # replicas evaluate different theta points (a line-search batch)
+        thetas.append(replica_theta(config_of(name)["theta"], rank))
+        Ks.append(k if k is not None else max(1, args.batch))
+    mixed = len(models) > 1
+    if not mixed:
+        # Q_c, Q_prior and Q_c's block inverses of every point stay resident
+        m = models[0]
+        per = (m.Qc.buf.numel() + m.Qp.buf.numel() + m.nt * m.b * m.b) * 8
+        free, _ = torch.cuda.mem_get_info(dev)
+        Ks[0] = int(max(1, min(Ks[0], (free - (8 << 30)) // per + 1)))
+    units = sum(Ks)
+    model = models[0]
 
     peak = measured_fp64_peak(torch, dev)
 
@@ -252,29 +374,43 @@ def run_ours(args):
         if world > 1:
             torch.distributed.barrier()
 
-    K = max(1, args.batch)
+    def step_jobs(step):
+        return [(m, step_points(th, step, k)) for m, th, k in zip(models, thetas, Ks)]
 
-    def step_thetas(step):
-        return step_points(theta, step, K)
+    def run_step(step, precision=None):
+        jobs = step_jobs(step)
+        if mixed:
+            return adjoint_group(jobs, precision or args.precision)
+        m, pts = jobs[0]
+        return [m.objective_adjoint_batched(pts, precision)]
 
-    # ---- warm-up
+    def checks():
+        return [c for m in models for c in m.last_check]
+
+    def work_sum():
+        return {k: sum(m.work[k] for m in models) for k in models[0].work}
+
+    # ---- warm-up, then further untimed steps while the autotuner is still
+    # trying candidates for a launch shape of the step (bounded)
     nwarm = max(args.warmup, 3)
     for s in range(nwarm):
-        model.objective_adjoint_batched(step_thetas(s))
+        run_step(s)
+    extra = 0
+    while lib.bta_tune_pending() > 0 and extra < 12:
+        run_step(nwarm + extra)
+        extra += 1
     barrier()
 
     # ---- one profiled step, events around every launch: the per-category
     # split and the dominant kernel category.  Only that category's launches
     # carry events in the timed region (events around all ~1400 launches of a
     # step cost ~2.5 %).
-    import ctypes
-
     pre_ms = (ctypes.c_double * 8)()
     pre_cnt = (ctypes.c_longlong * 8)()
     lib.bta_prof_read(None, None)
     lib.bta_prof_mask(0xFF)
     lib.bta_prof_enable(1)
-    model.objective_adjoint_batched(step_thetas(nwarm + 2 * args.steps))
+    run_step(nwarm + 2 * args.steps)
     lib.bta_prof_enable(0)
     lib.bta_prof_read(pre_ms, pre_cnt)
     # the 8-bit-slice GEMM's digit pre-pass counts towards the GEMM's time
@@ -288,21 +424,20 @@ def run_ours(args):
     lib.bta_prof_mask(1 if dom == 0 else (1 << 1) | (1 << 5))
     lib.bta_prof_enable(1)
     launches0 = lib.bta_launch_count()
-    work0 = dict(model.work)
-    step_th = [step_thetas(nwarm + s) for s in range(args.steps)]
+    work0 = work_sum()
     barrier()
     e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
     e0.record()
     fallbacks = 0
     resid_max = 0.0
     for s in range(args.steps):
-        model.objective_adjoint_batched(step_th[s])
-        fallbacks += sum(1 for c in model.last_check if c["fallback"])
-        resid_max = max([resid_max] + [max(c["residual_c"], c["residual_p"]) for c in model.last_check])
+        run_step(nwarm + s)
+        fallbacks += sum(1 for c in checks() if c["fallback"])
+        resid_max = max([resid_max] + [max(c["residual_c"], c["residual_p"]) for c in checks()])
     e1.record()
     barrier()
     launches = lib.bta_launch_count() - launches0
-    work = {k: model.work[k] - work0[k] for k in work0}
+    work = {k: v - work0[k] for k, v in work_sum().items()}
     lib.bta_prof_enable(0)
     ms_cat = (ctypes.c_double * 8)()
     cnt_cat = (ctypes.c_longlong * 8)()
@@ -310,14 +445,14 @@ def run_ours(args):
     lib.bta_prof_mask(0xFF)
     clocks = clock.stop()
     t_dev = max_over_ranks(e0.elapsed_time(e1) * 1e-3, world, dev)
-    value = job_rate(K * args.steps, world, t_dev)
+    value = job_rate(units * args.steps, world, t_dev)
 
-    # ---- single-point adjoint latency
+    # ---- single-point adjoint latency (first member)
     barrier()
     s0, s1 = torch.cuda.Event(True), torch.cuda.Event(True)
     s0.record()
     for s in range(args.steps):
-        model.objective_adjoint(step_thetas(s)[0])
+        model.objective_adjoint(step_points(thetas[0], s, 1)[0])
     s1.record()
     barrier()
     single_rate = args.steps / (s0.elapsed_time(s1) * 1e-3)
@@ -326,47 +461,61 @@ def run_ours(args):
     barrier()
     t0 = time.perf_counter()
     for s in range(args.steps):
-        th_host = [np.array(t) for t in step_thetas(nwarm + args.steps + s)]  # host buffers
-        fs, gs = model.objective_adjoint_batched(th_host)
+        out = run_step(nwarm + args.steps + s)  # host theta arrays in, host f / gradients out
     torch.cuda.synchronize()
     t_e2e = max_over_ranks(time.perf_counter() - t0, world, dev)
-    e2e = job_rate(K * args.steps, world, t_e2e)
-    f, g = fs[0], gs[0]
-    coef_bytes = model.slots[0].coef_host[0].numel() * 8
-    h2d = K * 2 * coef_bytes
-    d2h = K * ((5 + 3 * (2 * n - 1) * 4 + a * a) * 8) + 16
+    e2e = job_rate(units * args.steps, world, t_e2e)
+    f, g = out[0][0][0], out[0][1][0]
+    h2d = sum(k * 2 * m.slots[0].coef_host[0].numel() * 8 for m, k in zip(models, Ks))
+    d2h = sum(k * ((5 + 3 * (2 * m.nt - 1) * 4 * m.nv * m.nv + m.nb * m.nb) * 8) + 16 for m, k in zip(models, Ks))
 
-    # ---- plain FP64 finite differences (the reference's algorithm)
-    # accuracy of the reduced-precision selected inversion against FP64 at one
-    # point (outside every timed region)
+    # ---- accuracy of the reduced-precision selected inversion against FP64,
+    # per result, at one point of the first member (outside every timed region)
     accuracy = {"fallbacks_in_timed_region": fallbacks, "max_identity_residual": resid_max}
     if args.precision != "fp64":
-        fr, gr = model.objective_adjoint_batched([theta])
-        f64, g64 = model.objective_adjoint_batched([theta], precision="fp64")
-        accuracy["grad_rel_err_vs_fp64"] = float(np.linalg.norm(np.asarray(gr[0]) - np.asarray(g64[0]))
-                                                 / np.linalg.norm(np.asarray(g64[0])))
-        accuracy["f_rel_err_vs_fp64"] = abs(fr[0] - f64[0]) / abs(f64[0])
-    fd_rate = None
-    if args.fd_steps > 0:
-        barrier()
-        f0, f1 = torch.cuda.Event(True), torch.cuda.Event(True)
-        f0.record()
-        for _ in range(args.fd_steps):
-            model.objective_fd(theta)
-        f1.record()
-        barrier()
-        fd_rate = args.fd_steps / (f0.elapsed_time(f1) * 1e-3)
-    # the same stencil with its 2d+1 points factorised in batches (Gaussian)
-    fdb_rate = None
-    if args.fd_steps > 0 and model.gaussian:
-        barrier()
-        f0, f1 = torch.cuda.Event(True), torch.cuda.Event(True)
-        f0.record()
-        for _ in range(args.fd_steps):
-            model.objective_fd_batched(theta)
-        f1.record()
-        barrier()
-        fdb_rate = args.fd_steps / (f0.elapsed_time(f1) * 1e-3)
+        sl = model.slots[0]
+
+        def results(prec):
+            fr, gr = model.objective_adjoint_batched([thetas[0]], precision=prec)
+            dsel = torch.cat([torch.diagonal(sl.Qc.D, dim1=1, dim2=2).reshape(-1), torch.diagonal(sl.Qc.T)])
+            return fr[0], np.asarray(gr[0]), float(sl.scal[0]), sl.x.cpu().numpy(), dsel.cpu().numpy()
+
+        fr, gr, ldr, xr, sr = results(args.precision)
+        f64, g64, ld64, x64, s64 = results("fp64")
+        accuracy.update({
+            "grad_rel_err_vs_fp64": float(np.linalg.norm(gr - g64) / np.linalg.norm(g64)),
+            "f_rel_err_vs_fp64": abs(fr - f64) / abs(f64),
+            "logdet_qc_rel_err_vs_fp64": abs(ldr - ld64) / abs(ld64),
+            "solution_rel_err_vs_fp64": float(np.linalg.norm(xr - x64) / np.linalg.norm(x64)),
+            "selinv_diag_rel_err_vs_fp64": float(np.max(np.abs(sr - s64) / np.abs(s64))),
+            "note": ("the factorisations' Schur updates and the selected inversion's block products differ; "
+                     "POTRF, log-determinant sums and sweeps are FP64 in both") if args.factor_precision != "fp64"
+            else "factorisations, log-determinants and solves are FP64 in both; the selected inversion's "
+                 "block products differ",
+        })
+
+    # ---- plain FP64 finite differences (the reference's algorithm), warm:
+    # one untimed evaluation of each path, then --fd-steps timed repeats.
+    # A mixed batch: one point per member, weighted by its points per step.
+    def fd_rate(batched):
+        t_units = 0.0
+        for m, th, k in zip(models, thetas, Ks):
+            if batched and not m.gaussian:
+                return None
+            fn = m.objective_fd_batched if batched else m.objective_fd
+            fn(th)  # warm-up: slots, workspaces, task lists
+            barrier()
+            f0, f1 = torch.cuda.Event(True), torch.cuda.Event(True)
+            f0.record()
+            for _ in range(args.fd_steps):
+                fn(th)
+            f1.record()
+            barrier()
+            t_units += k * (f0.elapsed_time(f1) * 1e-3) / args.fd_steps
+        return units / t_units
+
+    fd_seq = fd_rate(False) if args.fd_steps > 0 else None
+    fd_bat = fd_rate(True) if args.fd_steps > 0 else None
 
     # ---- roofline of the dominant kernel category
     names = {0: "panel (tile-DAG BTA panel Cholesky)",
@@ -378,23 +527,21 @@ def run_ours(args):
     tot_flops = {0: work["factor"], 1: work["selinv_gemm"]}
     cat_ms = {0: ms_cat[0], 1: ms_cat[1] + ms_cat[5]}
     achieved = tot_flops[dom] / (cat_ms[dom] * 1e-3) / 1e12
-    traffic = None
-    tpath = os.path.join(REPO, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get(names[dom].split()[0])
-        except Exception:
-            traffic = None
+    # launch shape of the first member: block, arrow, matrices per launch
+    shape = (model.b, model.nb, 2 * Ks[0])
+    traffic, traffic_src = roofline_traffic(args.workload, names[dom].split()[0], shape)
     dom_peak, peak_src = peak, "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor pipe)"
     if dom == 1 and args.precision == "i8slice":
         # FP64-equivalent ceiling of 28 int8 digit products per product: the
         # dense int8 rate taken as twice the measured bf16 burst
         try:
             bf16 = float(json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))["bf16_tflops"])
+            src = "measured"
         except Exception:
-            bf16 = 1590.0
+            bf16, src = 1590.0, "fallback"
         dom_peak = 2 * bf16 / 28
-        peak_src = f"2 x measured bf16 burst ({bf16:.0f} TF/s) / 28 digit products (int8 ceiling, FP64-equivalent)"
+        peak_src = (f"2 x {src} bf16 burst ({bf16:.0f} TF/s) / 28 digit products "
+                    f"(int8 ceiling, FP64-equivalent)")
     roofline = {
         "bound": "tensor",
         "kernel": names[dom],
@@ -406,6 +553,7 @@ def run_ours(args):
         "avg_launch_ms": cat_ms[dom] / max(cnt_cat[dom], 1),
         "launches": int(cnt_cat[dom]),
         "traffic": traffic,
+        "traffic_source": traffic_src,
     }
     # per-category split of the profiled step (events around every launch)
     kernel_ms = {k: pre_ms[i] for i, k in enumerate(["panel", "gemm", "sweep", "trtri", "other", "slice"])}
@@ -413,12 +561,13 @@ def run_ours(args):
     cpu = None
     if rank == 0 and not args.no_cpu:
         try:
-            t_cpu, desc = cpu_sample(args.workload, args.cpu_nt)
+            t_cpu, desc, _ = cpu_sample(args.workload, args.cpu_nt)
             cpu = {"value": 1.0 / t_cpu, "unit": "evals/s", "cores": os.cpu_count(), "kind": "port", "sample": desc}
         except Exception as exc:  # reported, not fatal
             cpu = {"value": None, "unit": "evals/s", "cores": os.cpu_count(), "kind": "port", "sample": repr(exc)}
 
     if rank == 0:
+        cfg0 = config_of(mem[0][0])
         line = {
             "metric": METRIC,
             "value": value,
@@ -430,36 +579,46 @@ def run_ours(args):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else f"f64 + {args.precision} block products",
+            "dtype": "f64" if args.precision == "fp64" else (
+                f"f64 + {args.precision} selected-inversion products"
+                + (f" + {args.factor_precision} factor Schur updates" if args.factor_precision != "fp64" else "")),
             "data": "synthetic",
             "config": {
                 "workload": args.workload,
-                "ns": model.ns, "variates": model.nv, "block": b, "nt": n, "nb": a, "obs_per_step": cfg["no"],
-                "theta": list(cfg["theta"]),
-                "path": f"adjoint gradient, selected inversion in {args.precision} (factorisations, log-dets, solves "
-                        f"FP64); {K} theta points per step (line-search batch), theta moved "
-                        f"between steps; Q_c and Q_prior of all points factorised and selected-inverted together",
-                "theta_points_per_step": K,
+                "members": [{"workload": name, "block": m.b, "nt": m.nt, "nb": m.nb, "variates": m.nv,
+                             "ns": m.ns, "points_per_step": k} for (name, _), m, k in zip(mem, models, Ks)],
+                "obs_per_step": cfg0["no"],
+                "theta": list(cfg0["theta"]),
+                "path": f"adjoint gradient, selected inversion in {args.precision}, factorisations' Schur updates "
+                        f"in {args.factor_precision if args.precision != 'fp64' else 'fp64'} (POTRF, log-dets, "
+                        f"solves FP64); {units} theta points per step, theta moved between steps; Q_c and Q_prior of all "
+                        f"points factorised and selected-inverted together"
+                        + ("; members of different block sizes share every launch" if mixed else ""),
+                "theta_points_per_step": units,
                 "parallelism": f"replicas x{world}",
-                "likelihood": cfg.get("likelihood", "gaussian"),
-                "l2": f"inputs larger than L2 (BTA matrix {model.Qc.buf.numel() * 8 / 1e9:.1f} GB each)",
+                "likelihood": cfg0.get("likelihood", "gaussian"),
+                "l2": f"inputs larger than L2 (BTA matrix {model.Qc.buf.numel() * 8 / 1e9:.2f} GB each)",
             },
             "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
+            "autotune": {"decisions": _lib.tune_report(), "extra_warmup_steps": extra,
+                         "pending_after_warmup": int(lib.bta_tune_pending())},
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks,
             "mixed_accuracy": accuracy,
-            "fd_fp64_evals_per_s": fd_rate,
-            "fd_fp64_batched_stencil_evals_per_s": fdb_rate,
+            "fd_fp64_evals_per_s": fd_seq,
+            "fd_fp64_batched_stencil_evals_per_s": fd_bat,
+            "fd_timing": f"warm (one untimed evaluation first), {args.fd_steps} timed repeats per path",
             "adjoint_single_point_evals_per_s": single_rate,
-            "speedup_vs_fd_fp64": (value / fd_rate) if fd_rate else None,
+            "speedup_vs_fd_fp64": (value / fd_seq) if fd_seq else None,
+            "speedup_vs_fd_fp64_batched": (value / fd_bat) if fd_bat else None,
             # per-step work of the timed region over the profiled step's kernel times
             "bta_factor_tflops": tot_flops[0] / args.steps / max(pre_ms[0] * 1e-3, 1e-12) / 1e12,
             "bta_selinv_gemm_tflops": tot_flops[1] / args.steps / max((pre_ms[1] + pre_ms[5]) * 1e-3, 1e-12) / 1e12,
             "kernel_ms_source": "one profiled step before the timed region (events around every launch); "
                                 "in the timed region only the roofline kernel's launches carry events",
-            "newton_steps_per_point": (work["newton_steps"] / (K * args.steps)) if not model.gaussian else None,
+            "newton_steps_per_point": (work["newton_steps"] / (units * args.steps)) if not model.gaussian else None,
             "kernel_ms_per_step": kernel_ms,
             "f": f,
             "grad": list(map(float, g)),

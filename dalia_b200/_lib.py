@@ -44,6 +44,8 @@ SIGNATURES = {
     "bta_pobtas": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _int]),
     "bta_pobtaf_batched": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
                                   _c_void_p, _pi64]),
+    "bta_pobtaf_batched_ex": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                     _c_void_p, _c_void_p, _c_void_p, _pi64, _int]),
     "bta_pobtas_batched": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
                                   _c_void_p, _c_void_p, _int]),
     "bta_pobtasi_batched": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
@@ -69,6 +71,10 @@ SIGNATURES = {
     "bta_prof_mask": (_int, [_int]),
     "bta_prof_read": (_int, [_pdbl, ctypes.POINTER(ctypes.c_longlong)]),
     "bta_panel_task_list": (_int, [_int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _int, ctypes.POINTER(_int)]),
+    "bta_panel_task_list_ex": (_int, [_int, _c_void_p, _c_void_p, _c_void_p, _int, _c_void_p, _int,
+                                      ctypes.POINTER(_int)]),
+    "bta_tune_report": (_int, [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "bta_tune_pending": (_int, []),
     "bta_gather_coo": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _i64, _int,
                               _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p]),
     "bta_scatter_coo": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _c_void_p, _i64, _int,
@@ -206,3 +212,13 @@ def ptr(t) -> ctypes.c_void_p:
     if t is None:
         return _c_void_p(0)
     return _c_void_p(t.data_ptr())
+
+
+def tune_report():
+    """The autotuner's decisions so far, one line each (``bta_tune_report``)."""
+    lib = load()
+    n = ctypes.c_size_t(0)
+    lib.bta_tune_report(None, 0, ctypes.byref(n))
+    buf = ctypes.create_string_buffer(n.value + 1)
+    check(lib.bta_tune_report(buf, n.value + 1, ctypes.byref(n)), "tune_report")
+    return [ln for ln in buf.value.decode().splitlines() if ln]

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdalia_bta.so")
-SOURCES = ["gemm.cu", "gemm_tc.cu", "gemm_i8.cu", "panel.cu", "solve.cu", "solve_inv.cu", "selinv.cu", "bta.cu", "assemble.cu", "prof.cu", "noalloc.cu"]
+SOURCES = ["gemm.cu", "gemm_tc.cu", "gemm_i8.cu", "panel.cu", "solve.cu", "solve_inv.cu", "selinv.cu", "bta.cu", "assemble.cu", "prof.cu", "noalloc.cu", "tune.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

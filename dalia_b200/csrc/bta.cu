@@ -12,6 +12,7 @@
 #include "gemm.cuh"
 #include "panel.cuh"
 #include "prof.cuh"
+#include "tune.cuh"
 
 using namespace bta;
 
@@ -107,9 +108,10 @@ struct PanelSpec {
   double* Ttip = nullptr;
 };
 
-// Cached device task list of a panel batch with the given instance shapes.
-int get_tasks(bta_context* h, const std::vector<PanelInst>& insts, const int4** out, int* count) {
-  std::vector<int> key;
+// Cached device task list of a panel batch with the given instance shapes
+// and queue lookahead.
+int get_tasks(bta_context* h, const std::vector<PanelInst>& insts, int lookahead, const int4** out, int* count) {
+  std::vector<int> key{lookahead};
   for (const auto& I : insts) {
     key.push_back(I.b);
     key.push_back(I.a);
@@ -119,7 +121,7 @@ int get_tasks(bta_context* h, const std::vector<PanelInst>& insts, const int4** 
   auto it = h->tasks.find(key);
   if (it == h->tasks.end()) {
     std::vector<int4> t;
-    panel_tasks(insts, t);
+    panel_tasks(insts, t, lookahead);
     int4* d = nullptr;
     if (!t.empty()) {
       if (cudaMalloc(&d, t.size() * sizeof(int4)) != cudaSuccess) return BTA_ERR_ALLOC;
@@ -171,9 +173,26 @@ int run_panels(bta_context* h, const std::vector<PanelSpec>& specs, Carve& cv) {
       I.prv = cnt + off + (size_t)2 * I.nrows_t * I.nq;
       off += (size_t)3 * I.nrows_t * I.nq;
     }
+    // launch shape: instances, their block and arrow sizes, which terms the
+    // launch applies; candidates: queue lookahead x resident CTAs per SM
+    std::vector<long long> tkey{(long long)insts.size()};
+    for (const auto& I : insts)
+      tkey.push_back(((long long)I.b << 20) | ((long long)I.a << 4) | (I.L ? 1 : 0) | (I.Lprev ? 2 : 0) |
+                     (I.Abprev ? 4 : 0) | (I.Ttip ? 8 : 0));
+    const int occ = panel_ctas_per_sm();
+    if (occ < 0) return BTA_ERR_CUDA;
+    static const int kLook[3] = {PREV_LOOKAHEAD, 1, 4};
+    // only the launches that repeat within one factorisation (block columns
+    // with a previous-column term and a block below) are tuned
+    bool bulk = true;
+    for (const auto& I : insts) bulk = bulk && I.L != nullptr && I.Lprev != nullptr;
+    const int ncand = bulk ? 3 * std::min(occ, 2) : 1;
+    TuneLaunch tl("panel", tkey, ncand, h->stream);
+    const int lookahead = kLook[tl.choice() % 3];
+    const int grid = device_sm_count() * (occ - tl.choice() / 3);
     const int4* tasks;
     int ntasks;
-    int rc = get_tasks(h, insts, &tasks, &ntasks);
+    int rc = get_tasks(h, insts, lookahead, &tasks, &ntasks);
     if (rc) return rc;
     if (cudaMemsetAsync(cnt, 0, (cnt_total + 4) * sizeof(int), h->stream) != cudaSuccess) return BTA_ERR_CUDA;
     B.ninst = (int)insts.size();
@@ -182,7 +201,7 @@ int run_panels(bta_context* h, const std::vector<PanelSpec>& specs, Carve& cv) {
     B.counter = cnt + cnt_total;
     B.abort_flag = h->ctl;
     for (size_t k = 0; k < insts.size(); ++k) B.inst[k] = insts[k];
-    rc = cuda_rc(panel_launch(B, 0, h->stream));
+    rc = cuda_rc(panel_launch(B, grid, h->stream));
     if (rc) return rc;
   }
   return BTA_OK;
@@ -301,7 +320,19 @@ size_t bta_workspace_bytes(bta_handle_t h) { return h ? h->ws_bytes : 0; }
 
 int bta_pobtaf_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
                        double* const* D, double* const* L, double* const* Ab, double* const* T, int64_t* info) {
+  return bta_pobtaf_batched_ex(h, count, n, b, a, D, L, Ab, T, info, BTA_PREC_FP64);
+}
+
+int bta_pobtaf_batched_ex(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                          double* const* D, double* const* L, double* const* Ab, double* const* T, int64_t* info,
+                          int precision) {
   if (!h || count < 1 || !n || !b || !a || !D) return BTA_ERR_INVALID;
+  if (precision != BTA_PREC_FP64 && precision != BTA_PREC_TF32X3 && precision != BTA_PREC_I8SLICE)
+    return BTA_ERR_INVALID;
+  // FP64: the previous block column's Schur term runs inside the panel launch
+  // (dependency-free tile tasks); otherwise it is one grouped GEMM per block
+  // column in the requested arithmetic between the panel launches.
+  const bool split = precision != BTA_PREC_FP64;
   int64_t maxn = 0;
   size_t need = 0, need_tip = 0;
   for (int k = 0; k < count; ++k) {
@@ -333,7 +364,7 @@ int bta_pobtaf_batched(bta_handle_t h, int count, const int64_t* n, const int64_
       double* Li = hasL ? L[k] + i * bb : nullptr;
       double* Abi = a[k] > 0 ? Ab[k] + i * ab : nullptr;
       PanelSpec sp{Di, Li, Abi, (int)b[k], (int)a[k], ((long long)k << 40) + (long long)(i * b[k])};
-      if (i > 0) {
+      if (i > 0 && !split) {
         sp.Lprev = L[k] + (i - 1) * bb;
         sp.Abprev = a[k] > 0 ? Ab[k] + (i - 1) * ab : nullptr;
       }
@@ -350,6 +381,26 @@ int bta_pobtaf_batched(bta_handle_t h, int count, const int64_t* n, const int64_
     rc = run_panels(h, specs, cv);
     if (rc) return rc;
     if (!probs.empty() && gemm_launch(probs, s) != cudaSuccess) return BTA_ERR_CUDA;
+    if (split) {
+      // Schur term of block column i+1: D_{i+1} -= L_i L_i^T (lower half),
+      // Ab_{i+1} -= Ab_i L_i^T
+      std::vector<GemmProb> sch;
+      for (int k = 0; k < count; ++k) {
+        if (i >= n[k] - 1) continue;
+        const size_t bb = (size_t)b[k] * b[k], ab = (size_t)a[k] * b[k];
+        const int B_ = (int)b[k], A_ = (int)a[k];
+        double* Li = L[k] + i * bb;
+        GemmProb p = gemm_prob(D[k] + (i + 1) * bb, B_, B_, B_, 1.0, GC_LOWER);
+        gemm_add(p, Li, B_, Li, B_, B_, -1.0, 0);
+        sch.push_back(p);
+        if (a[k] > 0) {
+          GemmProb q = gemm_prob(Ab[k] + (i + 1) * ab, B_, A_, B_, 1.0);
+          gemm_add(q, Ab[k] + i * ab, B_, Li, B_, B_, -1.0, 0);
+          sch.push_back(q);
+        }
+      }
+      if (!sch.empty() && (rc = run_gemm(h, sch, precision))) return rc;
+    }
   }
   std::vector<PanelSpec> tips;
   for (int k = 0; k < count; ++k)
@@ -369,16 +420,101 @@ int bta_pobtaf(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, doubl
   return bta_pobtaf_batched(h, 1, &n, &b, &a, &D, &L, &Ab, &T, info);
 }
 
+// Whether a sweep of these instances is faster through block inverses made
+// here chunk by chunk (b^3/3 flops per block on the tensor cores, then n
+// bandwidth-bound steps of the persistent sweep) than through the tile-task
+// sweep (n ceil(b/64) dependent 64-row links per instance, instances in
+// parallel).  Model: ~10 us per link, ~2 TB/s for the tile sweep's reads;
+// ~20 TF/s for the block inverses, ~15 us per persistent step.
+bool sweep_by_inverses(int count, const int64_t* n, const int64_t* b, const int64_t* a) {
+  double chain = 0, tile_bytes = 0, inv_flops = 0, inv_bytes = 0;
+  int64_t maxn = 0;
+  for (int k = 0; k < count; ++k) {
+    const double bb = (double)b[k] * b[k];
+    chain = std::max(chain, (double)n[k] * ((b[k] + 63) / 64) * 10e-6);
+    tile_bytes += 8.0 * (1.5 * n[k] * bb + (double)n[k] * a[k] * b[k]);
+    inv_flops += (double)n[k] * bb * b[k] / 3.0;
+    inv_bytes += 8.0 * (2.0 * n[k] * bb);
+    maxn = std::max(maxn, n[k]);
+  }
+  const double t_tile = std::max(chain, tile_bytes / 2e12);
+  const double t_inv = inv_flops / 20e12 + inv_bytes / 5e12 + maxn * 15e-6;
+  return t_inv < t_tile;
+}
+
 int bta_pobtas_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
                        const double* const* D, const double* const* L, const double* const* Ab,
                        const double* const* T, double* const* rhs, int trans) {
   if (!h || count < 1 || count > SWEEP_MAXI || !n || !b || !a || !D || !rhs) return BTA_ERR_INVALID;
   if (trans != 0 && trans != 1) return BTA_ERR_INVALID;
-  size_t need = 4 * kAlign;
   for (int k = 0; k < count; ++k) {
     if (n[k] < 1 || b[k] < 1 || a[k] < 0 || !D[k] || !rhs[k] || (n[k] > 1 && (!L || !L[k])) ||
-        (a[k] > 0 && (!Ab || !T || !Ab[k] || !T[k])))
+        (a[k] > 0 && (!Ab || !T || !Ab[k] || !T[k])) || b[k] > INT32_MAX / 2)
       return BTA_ERR_INVALID;
+  }
+  if (sweep_by_inverses(count, n, b, a)) {
+    // block inverses of C steps at a time (about 1 GiB for all instances),
+    // each chunk then swept by one persistent launch
+    std::vector<int> ni(count), bi(count), ai(count), vlo(count, 0);
+    std::vector<const double*> Lk(count), Abk(count), Vk(count);
+    std::vector<double*> tinv(count), vbuf(count);
+    int64_t maxn = 0;
+    double per_step = 0;
+    size_t apart = 1;
+    for (int k = 0; k < count; ++k) {
+      ni[k] = (int)n[k];
+      bi[k] = (int)b[k];
+      ai[k] = (int)a[k];
+      Lk[k] = n[k] > 1 ? L[k] : nullptr;
+      Abk[k] = a[k] > 0 ? Ab[k] : nullptr;
+      maxn = std::max(maxn, n[k]);
+      per_step += 8.0 * b[k] * b[k];
+      apart = std::max<size_t>(apart, (size_t)n[k] * a[k]);
+    }
+    const int64_t C = std::max<int64_t>(1, std::min<int64_t>(maxn, (int64_t)((double)(1 << 30) / per_step)));
+    size_t need = 4 * kAlign + align_up((sweep_inv_work_total(count, ni.data(), bi.data(), ai.data()) + apart) * 8);
+    for (int k = 0; k < count; ++k) {
+      const size_t nq = (b[k] + 63) / 64;
+      need += align_up(C * nq * 4096 * 8) + align_up(C * (size_t)b[k] * b[k] * 8);
+    }
+    int rc = ensure_ws(h, need);
+    if (rc) return rc;
+    cudaStream_t s = h->stream;
+    Carve cv{h->ws};
+    double* work = cv.take<double>(sweep_inv_work_total(count, ni.data(), bi.data(), ai.data()) + apart);
+    for (int k = 0; k < count; ++k) {
+      const size_t nq = (b[k] + 63) / 64;
+      tinv[k] = cv.take<double>(C * nq * 4096);
+      vbuf[k] = cv.take<double>(C * (size_t)b[k] * b[k]);
+      Vk[k] = vbuf[k];
+    }
+    if (trans == 1)
+      for (int k = 0; k < count; ++k)
+        if (a[k] > 0 && arrow_backward(T[k], rhs[k], ni[k], bi[k], ai[k], s)) return BTA_ERR_CUDA;
+    for (int64_t s0 = 0; s0 < maxn; s0 += C) {
+      const int64_t s1 = std::min(maxn, s0 + C);
+      for (int k = 0; k < count; ++k) {
+        const int64_t e = std::min(s1, n[k]), cnt = e - s0;
+        if (cnt <= 0) continue;
+        const int64_t lo = trans == 0 ? s0 : n[k] - e;
+        const size_t bb = (size_t)b[k] * b[k];
+        if (diag_tile_inverses(D[k] + lo * bb, (int)cnt, bi[k], tinv[k], s)) return BTA_ERR_CUDA;
+        if (block_trtri(D[k] + lo * bb, tinv[k], 0, (int)cnt, bi[k], vbuf[k], s)) return BTA_ERR_CUDA;
+        vlo[k] = (int)lo;
+      }
+      if (sweep_inv_steps(count, ni.data(), bi.data(), ai.data(), Lk.data(), Abk.data(), Vk.data(), vlo.data(), rhs,
+                          trans, (int)s0, (int)s1, work, h->ctl, s))
+        return BTA_ERR_CUDA;
+    }
+    if (trans == 0)
+      for (int k = 0; k < count; ++k) {
+        double* part = work + sweep_inv_work_total(count, ni.data(), bi.data(), ai.data());
+        if (a[k] > 0 && arrow_forward(Ab[k], T[k], rhs[k], ni[k], bi[k], ai[k], part, s)) return BTA_ERR_CUDA;
+      }
+    return cuda_rc(cudaGetLastError());
+  }
+  size_t need = 4 * kAlign;
+  for (int k = 0; k < count; ++k) {
     const size_t nq = (b[k] + 63) / 64;
     need += align_up(n[k] * nq * 4096 * 8) + align_up((n[k] * nq + 4) * 4) + align_up((n[k] * a[k] + 1) * 8) +
             3 * kAlign;
@@ -443,27 +579,34 @@ int bta_pobtasi_batched_ex(bta_handle_t h, int count, const int64_t* n, const in
   return bta_pobtasi_batched_v(h, count, n, b, a, D, L, Ab, T, nullptr, precision);
 }
 
+// Blocks whose inverses one instance computes at a time when the caller does
+// not supply them: the inverses are made chunk by chunk as the backward
+// recurrence reaches them, so the workspace holds C blocks instead of n.
+inline int64_t inverse_chunk(int64_t n, int64_t b) {
+  const int64_t per = b * b * 8;
+  return std::max<int64_t>(1, std::min<int64_t>(n, (int64_t(512) << 20) / per));
+}
+
 int bta_pobtasi_batched_v(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
                           double* const* D, double* const* L, double* const* Ab, double* const* T,
                           const double* const* V, int precision) {
   if (!h || count < 1 || !n || !b || !a || !D) return BTA_ERR_INVALID;
-  if (V)
-    for (int k = 0; k < count; ++k)
-      if (!V[k]) return BTA_ERR_INVALID;
   if (precision != BTA_PREC_FP64 && precision != BTA_PREC_TF32X3 && precision != BTA_PREC_I8SLICE)
     return BTA_ERR_INVALID;
   // the block products go to the grouped GEMM of the requested arithmetic
   auto launch = [&](const std::vector<GemmProb>& pr) { return run_gemm(h, pr, precision); };
   size_t need = 8 * kAlign;
   int64_t maxn = 0;
+  std::vector<int64_t> chunk(count, 0);  // > 0: inverses computed here, chunk blocks at a time
   for (int k = 0; k < count; ++k) {
     if (n[k] < 1 || b[k] < 1 || a[k] < 0 || !D[k] || (n[k] > 1 && (!L || !L[k])) ||
         (a[k] > 0 && (!Ab || !T || !Ab[k] || !T[k])))
       return BTA_ERR_INVALID;
     const size_t nq = (b[k] + 63) / 64, nqa = (a[k] + 63) / 64;
     const size_t bb = (size_t)b[k] * b[k], ab = (size_t)a[k] * b[k];
-    // block inverses (tile inverses + full inverses) only when not supplied
-    need += (V ? 0 : align_up(n[k] * nq * 4096 * 8) + align_up(n[k] * bb * 8)) + 2 * align_up(bb * 8) +
+    if (!V || !V[k]) chunk[k] = inverse_chunk(n[k], b[k]);
+    // block inverses (tile inverses + full inverses of a chunk) only when not supplied
+    need += (chunk[k] ? align_up(chunk[k] * nq * 4096 * 8) + align_up(chunk[k] * bb * 8) : 0) + 2 * align_up(bb * 8) +
             align_up(ab * 8 + 8) + align_up(nqa * 4096 * 8 + 8) + align_up((size_t)a[k] * a[k] * 8 + 8) + 7 * kAlign;
     maxn = std::max(maxn, n[k]);
   }
@@ -473,13 +616,15 @@ int bta_pobtasi_batched_v(bta_handle_t h, int count, const int64_t* n, const int
   Carve cv{h->ws};
   struct W {
     double *tinv, *Linv, *G, *S, *Ga, *tinv_t, *Wt;
+    int64_t lo;  // first block of the chunk held in Linv (own inverses)
   };
   std::vector<W> w(count);
   for (int k = 0; k < count; ++k) {
     const size_t nq = (b[k] + 63) / 64, nqa = (a[k] + 63) / 64;
     const size_t bb = (size_t)b[k] * b[k], ab = (size_t)a[k] * b[k];
-    w[k].tinv = V ? nullptr : cv.take<double>(n[k] * nq * 4096);
-    w[k].Linv = V ? const_cast<double*>(V[k]) : cv.take<double>(n[k] * bb);
+    w[k].tinv = chunk[k] ? cv.take<double>(chunk[k] * nq * 4096) : nullptr;
+    w[k].Linv = chunk[k] ? cv.take<double>(chunk[k] * bb) : const_cast<double*>(V[k]);
+    w[k].lo = chunk[k] ? n[k] : 0;
     w[k].G = cv.take<double>(bb);
     w[k].S = cv.take<double>(bb);
     w[k].Ga = cv.take<double>(ab + 1);
@@ -488,10 +633,6 @@ int bta_pobtasi_batched_v(bta_handle_t h, int count, const int64_t* n, const int
   }
   std::vector<GemmProb> ptip;
   for (int k = 0; k < count; ++k) {
-    if (!V) {
-      if (diag_tile_inverses(D[k], (int)n[k], (int)b[k], w[k].tinv, s)) return BTA_ERR_CUDA;
-      if (block_trtri(D[k], w[k].tinv, 0, (int)n[k], (int)b[k], w[k].Linv, s)) return BTA_ERR_CUDA;
-    }
     if (a[k] > 0) {
       const int A_ = (int)a[k];
       if (diag_tile_inverses(T[k], 1, A_, w[k].tinv_t, s)) return BTA_ERR_CUDA;
@@ -509,10 +650,18 @@ int bta_pobtasi_batched_v(bta_handle_t h, int count, const int64_t* n, const int
       const int64_t i = n[k] - 1 - st;
       if (i < 0) continue;
       const size_t bb = (size_t)b[k] * b[k], ab = (size_t)a[k] * b[k];
+      if (chunk[k] && i < w[k].lo) {
+        // inverses of blocks [lo, i] (the factor blocks there are not yet
+        // overwritten: the recurrence runs from the last block down)
+        const int64_t lo = std::max<int64_t>(0, i + 1 - chunk[k]), cnt = i + 1 - lo;
+        if (diag_tile_inverses(D[k] + lo * bb, (int)cnt, (int)b[k], w[k].tinv, s)) return BTA_ERR_CUDA;
+        if (block_trtri(D[k] + lo * bb, w[k].tinv, 0, (int)cnt, (int)b[k], w[k].Linv, s)) return BTA_ERR_CUDA;
+        w[k].lo = lo;
+      }
       const bool hasL = i < n[k] - 1;
       double* Li = hasL ? L[k] + i * bb : nullptr;
       double* Abi = a[k] > 0 ? Ab[k] + i * ab : nullptr;
-      const double* Vi = w[k].Linv + i * bb;
+      const double* Vi = w[k].Linv + (i - w[k].lo) * bb;
       const int B_ = (int)b[k], A_ = (int)a[k];
       if (hasL) {
         GemmProb p = gemm_prob(w[k].G, B_, B_, B_, 0.0);
@@ -558,7 +707,13 @@ int bta_pobtasi(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, doub
 }
 
 int bta_panel_task_list(int count, const int* b, const int* a, const int* flags, int* out, int cap, int* n_out) {
-  if (count < 1 || count > PANEL_MAXI || !b || !a || !flags || !n_out || cap < 0 || (cap > 0 && !out))
+  return bta_panel_task_list_ex(count, b, a, flags, PREV_LOOKAHEAD, out, cap, n_out);
+}
+
+int bta_panel_task_list_ex(int count, const int* b, const int* a, const int* flags, int lookahead, int* out, int cap,
+                           int* n_out) {
+  if (count < 1 || count > PANEL_MAXI || !b || !a || !flags || !n_out || cap < 0 || (cap > 0 && !out) ||
+      lookahead < 1)
     return BTA_ERR_INVALID;
   static double present;  // stands for a matrix block: only null / non-null matters here
   std::vector<PanelInst> insts;
@@ -578,7 +733,7 @@ int bta_panel_task_list(int count, const int* b, const int* a, const int* flags,
     insts.push_back(I);
   }
   std::vector<int4> t;
-  panel_tasks(insts, t);
+  panel_tasks(insts, t, lookahead);
   *n_out = (int)t.size();
   if ((int)t.size() > cap) return BTA_ERR_INVALID;
   for (size_t i = 0; i < t.size(); ++i) {
@@ -614,7 +769,7 @@ int bta_pobtas_inv_batched(bta_handle_t h, int count, const int64_t* n, const in
   if (!h || count < 1 || !n || !b || !a || !V || !rhs || (trans != 0 && trans != 1)) return BTA_ERR_INVALID;
   std::vector<int> ni(count), bi(count), ai(count);
   std::vector<const double*> Lk(count), Abk(count), Tk(count);
-  size_t need = kAlign;
+  size_t need = kAlign, apart = 1;
   for (int k = 0; k < count; ++k) {
     if (n[k] < 1 || b[k] < 1 || a[k] < 0 || !V[k] || !rhs[k] || (n[k] > 1 && (!L || !L[k])) ||
         (a[k] > 0 && (!Ab || !T || !Ab[k] || !T[k])) || b[k] > INT32_MAX / 2)
@@ -625,12 +780,13 @@ int bta_pobtas_inv_batched(bta_handle_t h, int count, const int64_t* n, const in
     Lk[k] = n[k] > 1 ? L[k] : nullptr;
     Abk[k] = a[k] > 0 ? Ab[k] : nullptr;
     Tk[k] = a[k] > 0 ? T[k] : nullptr;
-    need += sweep_inv_work(ni[k], bi[k], ai[k]) * sizeof(double);
+    apart = std::max<size_t>(apart, (size_t)n[k] * a[k]);
   }
+  need += (sweep_inv_work_total(count, ni.data(), bi.data(), ai.data()) + apart) * sizeof(double);
   int rc = ensure_ws(h, align_up(need));
   if (rc) return rc;
   return sweep_inv_batched(count, ni.data(), bi.data(), ai.data(), Lk.data(), Abk.data(), Tk.data(), V, rhs, trans,
-                           reinterpret_cast<double*>(h->ws), h->stream)
+                           reinterpret_cast<double*>(h->ws), h->ctl, h->stream)
              ? BTA_ERR_CUDA
              : BTA_OK;
 }

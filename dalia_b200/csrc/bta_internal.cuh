@@ -38,12 +38,22 @@ int arrow_forward(const double* Ab, const double* T, double* x, int n, int b, in
 int arrow_backward(const double* T, double* x, int n, int b, int a, cudaStream_t s);
 
 // Sweeps with precomputed block inverses V (solve_inv.cu): count instances,
-// x[k] of length n[k] b[k] + a[k]; work holds sweep_inv_work(n[k], b[k], a[k]) doubles
-// per instance.
+// x[k] of length n[k] b[k] + a[k].  sweep_inv_steps runs steps [s0, s1) in
+// processing order (forward: block i = s; backward: block i = n - 1 - s) as
+// one persistent cooperative launch per PS chunk of instances, with V[k]
+// holding the inverse of block vlo[k] (vlo == nullptr: 0) and those after
+// it; work holds sweep_inv_work_total(...) doubles.  The arrowhead steps are
+// not included.  sweep_inv_batched is a whole sweep with every block inverse
+// supplied, arrowhead included; its work also holds max_k n[k] a[k] more
+// doubles.  abort_flag is raised when a grid barrier's bounded wait runs out.
 size_t sweep_inv_work(int n, int b, int a);
+size_t sweep_inv_work_total(int count, const int* n, const int* b, const int* a);
+int sweep_inv_steps(int count, const int* n, const int* b, const int* a, const double* const* L,
+                    const double* const* Ab, const double* const* V, const int* vlo, double* const* x, int trans,
+                    int s0, int s1, double* work, int* abort_flag, cudaStream_t s);
 int sweep_inv_batched(int count, const int* n, const int* b, const int* a, const double* const* L,
                       const double* const* Ab, const double* const* T, const double* const* V, double* const* x,
-                      int trans, double* work, cudaStream_t s);
+                      int trans, double* work, int* abort_flag, cudaStream_t s);
 
 // Full inverses of the lower-triangular factor blocks D[i0..i1) -> out
 // (i1-i0 blocks of b x b, zeros above the diagonal); tile_inv holds the

@@ -522,7 +522,8 @@ void prev_tasks(const std::vector<PanelInst>& insts, int c, std::vector<int4>& t
 
 }  // namespace
 
-void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks) {
+void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks, int lookahead) {
+  lookahead = std::max(1, lookahead);
   int max_nq = 0;
   for (const auto& I : insts) max_nq = std::max(max_nq, I.nq);
   int prev_done = -1;  // last column whose previous-column tasks are queued
@@ -534,7 +535,7 @@ void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks) 
       tasks.push_back(make_int4(ii, TASK_AGG_DIAG, r, r));
       if (r + 1 < I.nq) tasks.push_back(make_int4(ii, TASK_AGG_SUB, r + 1, r));
     }
-    while (prev_done < std::min(r + PREV_LOOKAHEAD, max_nq - 1)) prev_tasks(insts, ++prev_done, tasks);
+    while (prev_done < std::min(r + lookahead, max_nq - 1)) prev_tasks(insts, ++prev_done, tasks);
     for (int ii = 0; ii < (int)insts.size(); ++ii) {
       const PanelInst& I = insts[ii];
       if (r >= I.nq) continue;
@@ -550,14 +551,21 @@ void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks) 
     if (insts[ii].Ttip != nullptr) tasks.push_back(make_int4(ii, TASK_TIP, 0, 0));
 }
 
-int panel_grid_size() {
+int panel_ctas_per_sm() {
   const int e = ensure_smem_attr(reinterpret_cast<const void*>(panel_kernel), (int)SMEM_BYTES);
   if (e != cudaSuccess) return -e;
-  // one resident CTA per SM at this shared-memory size (the occupancy query
-  // is cheap next to a panel launch, and answers for the current device)
+  // resident CTAs per SM at this shared-memory and register use (the
+  // occupancy query is cheap next to a panel launch, and answers for the
+  // current device)
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel, THREADS, SMEM_BYTES);
-  return std::max(2, device_sm_count() * std::max(1, occ));
+  return std::max(1, occ);
+}
+
+int panel_grid_size() {
+  const int occ = panel_ctas_per_sm();
+  if (occ < 0) return occ;
+  return std::max(2, device_sm_count() * occ);
 }
 
 int panel_launch(const PanelBatch& batch, int grid, cudaStream_t stream) {

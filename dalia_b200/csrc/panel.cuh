@@ -62,7 +62,7 @@ struct PanelBatch {
 enum : int { TASK_AGG_DIAG = 3, TASK_AGG_SUB = 4, TASK_AGG_TRSM = 5, TASK_TIP = 6, TASK_PREV = 7 };
 
 // Tile columns by which the previous-column tasks run ahead of the tiles'
-// own tasks in the queue.
+// own tasks in the queue (default; the autotuner tries others).
 constexpr int PREV_LOOKAHEAD = 2;
 
 // Number of tile rows of a panel (diag rows, lower rows, arrow rows).
@@ -72,12 +72,14 @@ inline int panel_rows(int b, int a, bool has_L) {
 }
 
 // Queue tasks (every tile except those the chain finishes) of all instances.
-void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks);
+void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks, int lookahead = PREV_LOOKAHEAD);
 
 // Launch one panel batch.  The counters of every instance, batch.counter[0..1]
 // and the abort flag must be zero-initialised by the caller.
 int panel_launch(const PanelBatch& batch, int grid, cudaStream_t stream);
 
 int panel_grid_size();
+// CTAs per SM that fit (the largest grid is panel_grid_size()).
+int panel_ctas_per_sm();
 
 }  // namespace bta

@@ -167,8 +167,7 @@ class _Slot:
         self.gvec = torch.zeros(nobs, **f64)  # y - e exp(eta)
         self.hvec = torch.zeros(nobs, **f64)
         self.Sc = None  # copy of Q_c's factor, selected-inverted (allocated on first use)
-        self.Vc = None  # inverses of the diagonal factor blocks of Q_c / Q_prior (allocated on first use)
-        self.Vp = None
+        self.Vc = None  # inverses of the diagonal factor blocks of Q_c (allocated on first use)
         # one pinned host buffer per assembly so that queued copies never race
         self.coef_host = [torch.zeros(nb4, dtype=torch.float64).pin_memory() for _ in range(2)]
         self.coef_dev = [torch.zeros(nb4, **f64) for _ in range(2)]
@@ -179,20 +178,29 @@ class SpatioTemporalModel:
     likelihood, evaluated on one GPU."""
 
     def __init__(self, prob, priors=None, fe_prec=1e-3, eps_gradient_f=1e-3, eps_inner_iteration=1e-3,
-                 inner_iteration_max_iter=50, device=None, selinv_precision="fp64", mixed_tolerance=1e-8):
+                 inner_iteration_max_iter=50, device=None, selinv_precision="fp64", mixed_tolerance=1e-8,
+                 factor_precision="fp64"):
         """selinv_precision: arithmetic of the selected inversions behind the
         adjoint gradient: "fp64", "tf32x3" (FP32-class block products on the
         tcgen05 tensor cores) or "i8slice" (8-bit digit products accumulated
-        exactly in INT32 on the tensor cores, ~1e-10 relative); the
-        factorisations, log-determinants and solves stay FP64.  Every adjoint evaluation checks its selected inverses through
-        the identity <S, Q> = dim(Q) over the BTA pattern; a "tf32x3" point
-        whose relative residual exceeds mixed_tolerance is recomputed in FP64.
-        The residuals of the last evaluation are in ``last_check``."""
+        exactly in INT32 on the tensor cores, ~1e-10 relative).
+        factor_precision: arithmetic of the factorisations' previous-column
+        Schur updates in a reduced-precision adjoint evaluation ("fp64" or
+        "i8slice"; the diagonal-block POTRF, the triangular solves, the
+        log-determinants and the sweeps stay FP64, and the plain f / FD paths
+        always factor in FP64).  Every adjoint evaluation checks its selected
+        inverses through the identity <S, Q> = dim(Q) over the BTA pattern; a
+        reduced-precision point whose relative residual exceeds
+        mixed_tolerance is recomputed entirely in FP64.  The residuals of the
+        last evaluation are in ``last_check``."""
         import torch
 
         if selinv_precision not in _PRECISIONS:
             raise ValueError(f"selinv_precision must be one of {sorted(_PRECISIONS)}")
+        if factor_precision not in ("fp64", "i8slice"):
+            raise ValueError("factor_precision must be 'fp64' or 'i8slice'")
         self.selinv_precision = selinv_precision
+        self.factor_precision = factor_precision
         self.mixed_tol = float(mixed_tolerance)
         self.last_check = []
 
@@ -448,17 +456,21 @@ class SpatioTemporalModel:
         T = ptrs(*[p[3].value for p in P])
         return k, n, b, a, D, L, Ab, T
 
-    def factor_batched(self, mats):
-        """All matrices factored together, block column by block column."""
+    def factor_batched(self, mats, precision="fp64"):
+        """All matrices factored together, block column by block column;
+        precision: arithmetic of the previous-column Schur updates."""
         self.work["factor"] += sum(factor_flops(m.n, m.b, m.a) for m in mats)
         k, n, b, a, D, L, Ab, T = self._batched_args(mats)
-        self._check(self.lib.bta_pobtaf_batched(self.h.bind_stream(), k, n, b, a, D, L, Ab, T, None),
-                    "pobtaf_batched")
+        self._check(self.lib.bta_pobtaf_batched_ex(self.h.bind_stream(), k, n, b, a, D, L, Ab, T, None,
+                                                   _PRECISIONS[precision]), "pobtaf_batched")
 
     def selinv_batched(self, mats, precision="fp64", Vs=None):
+        """Selected inversions of all matrices together; Vs (optional, entries
+        may be None) supplies the inverses of their diagonal factor blocks,
+        which the library otherwise computes chunk by chunk."""
         self.work["selinv_gemm"] += sum(selinv_gemm_flops(m.n, m.b, m.a) for m in mats)
         k, n, b, a, D, L, Ab, T = self._batched_args(mats)
-        V = None if Vs is None else (ctypes.c_void_p * k)(*[v.data_ptr() for v in Vs])
+        V = None if Vs is None else (ctypes.c_void_p * k)(*[None if v is None else v.data_ptr() for v in Vs])
         self._check(self.lib.bta_pobtasi_batched_v(self.h.bind_stream(), k, n, b, a, D, L, Ab, T, V,
                                                    _PRECISIONS[precision]), "pobtasi_batched")
 
@@ -477,18 +489,46 @@ class SpatioTemporalModel:
                     "pobtas_inv_batched")
 
     def _slot_inverses(self, sl):
+        """Inverses of Q_c's diagonal factor blocks (n b^2 doubles), kept for
+        the triangular sweeps and the selected inversion.  Q_prior needs no
+        sweep: its selected inversion computes its block inverses chunk by
+        chunk, so they never occupy n b^2 at once."""
         import torch
 
         if sl.Vc is None:
-            nbb = self.nt * self.b * self.b
-            sl.Vc = torch.empty(nbb, dtype=torch.float64, device=self.device)
-            sl.Vp = torch.empty(nbb, dtype=torch.float64, device=self.device)
-        return sl.Vc, sl.Vp
+            sl.Vc = torch.empty(self.nt * self.b * self.b, dtype=torch.float64, device=self.device)
+        return sl.Vc
 
     def logdet_to(self, M: BTAMatrix, out):
         D, _, _, T = M.ptrs()
         self._check(self.lib.bta_logdet(self.h.bind_stream(), M.n, M.b, M.a, D, T, 1 if M.a else 0, _lib.ptr(out),
                                         None), "logdet")
+
+    def _inverses_fit(self, sls):
+        """Whether the slots' Q_c block inverses are (or can be made)
+        resident: n b^2 doubles per slot, kept for later use."""
+        import torch
+
+        missing = sum(1 for sl in sls if sl.Vc is None)
+        if missing == 0:
+            return True
+        free, _ = torch.cuda.mem_get_info(self.device)
+        return missing * self.nt * self.b * self.b * 8 + (4 << 30) < free
+
+    def solve_in_place(self, sls, xs):
+        """x <- Q_c^{-1} x for the factored Q_c of every slot: both triangular
+        sweeps through the inverses of the diagonal factor blocks (computed
+        once for both sweeps) when they fit in memory and the batch is small,
+        else the library's sweep (which picks its own method)."""
+        mats = [sl.Qc for sl in sls]
+        if len(sls) <= 2 and self._inverses_fit(sls):
+            Vs = [self._slot_inverses(sl) for sl in sls]
+            self.block_inverses(mats, Vs)
+            self.sweep_inv_batched(mats, Vs, xs, 0)
+            self.sweep_inv_batched(mats, Vs, xs, 1)
+        else:
+            self.sweep_batched(mats, xs, 0)
+            self.sweep_batched(mats, xs, 1)
 
     def sweep(self, M: BTAMatrix, x, trans):
         D, L, Ab, T = M.ptrs()
@@ -534,8 +574,7 @@ class SpatioTemporalModel:
             # rhs = -Q_prior x + A^T grad(lik) at x = 0, eta = 0  ->  sum_v tau_v A_v^T y_v
             self._gauss_rhs(theta, sl)
             sl.x.copy_(sl.rhs)
-            self.sweep(sl.Qc, sl.x, 0)
-            self.sweep(sl.Qc, sl.x, 1)
+            self.solve_in_place([sl], [sl.x])
             self.dot_to(sl.rhs, sl.x, sl.scal[1:2])  # mu^T Q_c mu = b^T mu
             self.assemble_prior_bt(theta, sl)
             self.factor(sl.Qp)
@@ -599,14 +638,31 @@ class SpatioTemporalModel:
             fs.append(float(f))
         return fs
 
-    def objective_fd_batched(self, theta, max_points=16):
+    def points_that_fit(self, want, reserve_bytes=6 << 30):
+        """How many theta points (of ``want``) can keep their device state --
+        Q_c, Q_prior and their vectors -- at once: the slots that exist plus
+        those the free device memory holds beyond ``reserve_bytes`` of
+        library workspace."""
+        import torch
+
+        have = len(self.slots)
+        if want <= have:
+            return want
+        free, _ = torch.cuda.mem_get_info(self.device)
+        per = (self.Qc.buf.numel() + self.Qp.buf.numel() + 8 * self.N + 4 * self.nobs) * 8
+        return int(max(1, min(want, have + max(0, free - reserve_bytes) // per)))
+
+    def objective_fd_batched(self, theta, max_points=None):
         """The reference's central-difference objective (``dalia.py:513-601``)
         with the 2d+1 stencil points evaluated in batches of up to
-        max_points (Gaussian likelihoods); the same values as
-        ``objective_fd``."""
+        max_points (Gaussian likelihoods; default: as many as device memory
+        holds, all 2d+1 when they fit -- one batched factorisation of the
+        2(2d+1) matrices); the same values as ``objective_fd``."""
         theta = np.asarray(theta, dtype=np.float64)
         d = theta.size
         nf = 2 * d + 1
+        if max_points is None:
+            max_points = self.points_that_fit(min(nf, 32))
         tm = np.repeat(theta.reshape(-1, 1), nf, axis=1)
         tm[:, 1:1 + d] += self.eps * np.eye(d)
         tm[:, d + 1:nf] -= self.eps * np.eye(d)
@@ -620,7 +676,7 @@ class SpatioTemporalModel:
             fv[idx] = self.evaluate_f_batched([tm[:, i] for i in idx])
         return fv[0], (fv[1:1 + d] - fv[d + 1:nf]) / (2 * self.eps)
 
-    def hessian_fd(self, theta, eps_hessian_f=5e-3, max_points=16):
+    def hessian_fd(self, theta, eps_hessian_f=5e-3, max_points=None):
         """Finite-difference Hessian of f (``DALIA._evaluate_hessian_f``,
         ``dalia.py:767-910``): f at theta, at theta +- eps e_i and at
         theta +- eps e_i +- eps e_j (i < j), 1 + 2d + 2d(d-1) points.  Gaussian
@@ -645,6 +701,8 @@ class SpatioTemporalModel:
                     slot_of[(i, j, si, sj)] = len(pts)
                     pts.append(theta + si * E[i] + sj * E[j])
         if self.gaussian:
+            if max_points is None:
+                max_points = self.points_that_fit(min(len(pts), 32))
             fv = []
             for c0 in range(0, len(pts), max_points):
                 fv += self.evaluate_f_batched(pts[c0:c0 + max_points])
@@ -716,56 +774,82 @@ class SpatioTemporalModel:
                  - mu^T db - d log p(theta) - d lik0,
         with tr(S dQ_st) and mu^T dQ_st mu contracted block by block against
         the Kronecker factors (c0, g1, g2, g3) and S = Q^{-1} on the BTA
-        pattern.  For a non-Gaussian likelihood see ``_adjoint_poisson_batched``."""
+        pattern.  The forward half (``adjoint_forward``: assembly,
+        factorisations, log-determinants, latent mean) and the backward half
+        (``adjoint_backward``: selected inversions and contractions) run back
+        to back.  For a non-Gaussian likelihood see ``_poisson_forward``."""
+        tok = self.adjoint_forward(thetas, precision, check=False)
+        return self.adjoint_backward(tok)
+
+    def adjoint_forward(self, thetas, precision=None, check=True):
+        """Forward half of the adjoint gradient at K theta points: f(theta)
+        with everything the backward half reuses left on the device (the
+        factors of Q_c and Q_prior, the inverses of their diagonal factor
+        blocks, the latent mean).  Returns a token for ``adjoint_backward``
+        and ``f_device``; check=True synchronises and raises on a matrix
+        that is not positive definite.  A later forward on this model
+        invalidates the token (the backward then recomputes the forward)."""
         precision = self.selinv_precision if precision is None else precision
-        if not self.gaussian:
-            return self._adjoint_poisson_batched(thetas, precision)
+        if precision not in _PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
         thetas = [np.asarray(t, dtype=np.float64) for t in thetas]
+        if not self.gaussian:
+            self._poisson_forward(thetas)
+        else:
+            self._gauss_forward(thetas, precision)
+        self._fwd_gen = getattr(self, "_fwd_gen", 0) + 1
+        tok = {"gen": self._fwd_gen, "thetas": thetas, "precision": precision, "fs": None}
+        self._fwd_token = tok
+        if check:
+            self.status()
+        if not self.gaussian:
+            tok["fs"] = [self._f_poisson(sl, th) for sl, th in zip(self.slots, thetas)]
+        return tok
+
+    def f_device(self, tok):
+        """f at the token's points as a device tensor (K,), without a host
+        synchronisation for Gaussian likelihoods."""
+        import torch
+
+        if tok["fs"] is not None:
+            return torch.tensor(tok["fs"], dtype=torch.float64, device=self.device)
+        self._require_live(tok)
+        K = len(tok["thetas"])
+        parts = torch.stack([self.slots[j].scal[:3] for j in range(K)])
+        c = torch.tensor([float(self.log_prior_theta(th) + self.lik0(th)) for th in tok["thetas"]],
+                         dtype=torch.float64, device=self.device)
+        return 0.5 * parts[:, 0] - 0.5 * parts[:, 1] - 0.5 * parts[:, 2] - c
+
+    def _require_live(self, tok):
+        if getattr(self, "_fwd_token", None) is not tok:
+            raise RuntimeError("the device state of this forward evaluation was overwritten by a later one")
+
+    def adjoint_backward(self, tok):
+        """Backward half: (f, gradient) at the token's points from the
+        selected inversions of Q_c and Q_prior and their contractions with
+        dQ/dtheta (block inner products against the Kronecker factors, the
+        quadratic and likelihood terms from the forward's latent mean).  A
+        token whose device state was overwritten is recomputed first.  The
+        selected inversion overwrites the factors, so the token is used up."""
+        if getattr(self, "_fwd_token", None) is not tok:
+            tok = self.adjoint_forward(tok["thetas"], tok["precision"], check=False)
+        self._fwd_token = None
+        if not self.gaussian:
+            return self._poisson_backward(tok)
+        return self._gauss_backward(tok)
+
+    def _gauss_forward(self, thetas, precision="fp64"):
+        _gauss_forward_group([(self, thetas)], self.factor_precision if precision != "fp64" else "fp64")
+
+    def _gauss_backward(self, tok):
+        return _gauss_backward_group([(self, tok)])[0]
+
+    def _gauss_gradients(self, thetas, precision):
+        """Host half of the Gaussian backward: f and the gradient of every
+        point from the scalars and block contractions on the device."""
         K = len(thetas)
-        n, a, ns, nv = self.nt, self.nb, self.ns, self.nv
-        stream = self._stream()
-        sls = [self.slot(j) for j in range(K)]
-        pat = (_lib.ptr(self.u_rowptr), _lib.ptr(self.u_col), _lib.ptr(self.u_vals4))
-        _lib.check(self.lib.bta_reset_status(self.h.bind_stream()), "reset")
-        for sl, th in zip(sls, thetas):
-            self._gauss_conditional(th, sl)
-            self.assemble_prior_bt(th, sl)
-        self.factor_batched([sl.Qc for sl in sls] + [sl.Qp for sl in sls])
-        # inverses of the diagonal factor blocks: the sweeps become n dependent
-        # matrix-vector steps, and the selected inversions reuse them
-        Vc = [self._slot_inverses(sl)[0] for sl in sls]
-        Vp = [self._slot_inverses(sl)[1] for sl in sls]
-        self.block_inverses([sl.Qc for sl in sls] + [sl.Qp for sl in sls], Vc + Vp)
-        for sl, th in zip(sls, thetas):
-            self.logdet_to(sl.Qc, sl.scal[0:1])
-            self.logdet_to(sl.Qp, sl.scal[2:3])
-            self._gauss_rhs(th, sl)
-            sl.x.copy_(sl.rhs)
-        self.sweep_inv_batched([sl.Qc for sl in sls], Vc, [sl.x for sl in sls], 0)
-        for sl in sls:
-            self.dot_to(sl.x, sl.x, sl.scal[1:2])  # b^T Q^-1 b = |L^-1 b|^2
-        self.sweep_inv_batched([sl.Qc for sl in sls], Vc, [sl.x for sl in sls], 1)  # mu
-        for sl in sls:
-            # per variate |A_v mu|^2 and (A_v mu)^T y_v; mu^T (E_tt' (x) K) mu per sub-block
-            self.spmv(self.A_rowptr, self.A_col, self.A_val, self.nobs, sl.x, sl.eta)
-            for j, (lo, hi) in enumerate(self.var_ranges):
-                self.dot_to(sl.eta[lo:hi], sl.eta[lo:hi], sl.vscal[3 * j + 1:3 * j + 2])
-                self.dot_to(sl.eta[lo:hi], self.y[lo:hi], sl.vscal[3 * j + 2:3 * j + 3])
-            self._check(self.lib.bta_block_quad_mv(stream, n, ns, nv, *pat, _lib.ptr(sl.x), _lib.ptr(sl.quad_st)),
-                        "block_quad")
-        # selected inverses and their contractions
-        self.selinv_batched([sl.Qc for sl in sls] + [sl.Qp for sl in sls], precision, Vc + Vp)
-        for sl in sls:
-            Dc, Lc, _, _ = sl.Qc.ptrs()
-            Dp, Lp, _, _ = sl.Qp.ptrs()
-            for (Dm, Lm, out) in ((Dc, Lc, sl.inner_c), (Dp, Lp, sl.inner_p)):
-                self._check(self.lib.bta_block_inner_mv(stream, n, ns, nv, *pat, Dm, Lm, _lib.ptr(out)), "block_inner")
-            for j in range(len(self.var_ranges)):
-                self._check(self.lib.bta_gather_dot(stream, self.nent, _lib.ptr(self.ent_dst),
-                                                    _lib.ptr(self.ata_w_var[j]), _lib.ptr(sl.Qc.buf),
-                                                    _lib.ptr(self.part), self.nparts,
-                                                    _lib.ptr(sl.vscal[3 * j:3 * j + 1])), "gather_dot")
-        self.status()
+        n = self.nt
+        sls = self.slots[:K]
         mult = np.ones((2 * n - 1, 1))
         mult[n:] = 2.0  # each sub-diagonal block appears twice in the symmetric matrix
         prior_idx = [k for k in range(len(self.theta_keys)) if k not in self.tau_idx]
@@ -898,8 +982,7 @@ class SpatioTemporalModel:
                 self.spmv(self.AT_rowptr, self.AT_col, self.AT_val, self.N, sl.gvec, sl.rhs)
                 self._check(self.lib.bta_axpby(s, self.N, -1.0, _lib.ptr(sl.qpx), 1.0, _lib.ptr(sl.rhs)), "axpby")
                 sl.upd.copy_(sl.rhs)
-            self.sweep_batched([sls[j].Qc for j in active], [sls[j].upd for j in active], 0)
-            self.sweep_batched([sls[j].Qc for j in active], [sls[j].upd for j in active], 1)
+            self.solve_in_place([sls[j] for j in active], [sls[j].upd for j in active])
             for j in active:
                 self.dot_to(sls[j].upd, sls[j].upd, sls[j].scal[6:7])
             self.status()
@@ -932,7 +1015,19 @@ class SpatioTemporalModel:
         self._newton([sl], [theta])
         return self._f_poisson(sl, theta)
 
-    def _adjoint_poisson_batched(self, thetas, precision="fp64"):
+    def _poisson_forward(self, thetas):
+        """Forward half for the Poisson likelihood: the Newton iteration of
+        every point to its mode (``_newton``), warm-started from the current
+        mode of slot 0; leaves Q_c (factored at the mode), the BT factor of
+        Q_prior and the scalars of f on the device."""
+        K = len(thetas)
+        sls = [self.slot(j) for j in range(K)]
+        for sl in sls[1:]:
+            sl.x.copy_(sls[0].x)  # warm start every point from the current mode
+        _lib.check(self.lib.bta_reset_status(self.h.bind_stream()), "reset")
+        self._newton(sls, thetas)
+
+    def _poisson_backward(self, tok):
         """(f, gradient) at K theta points for the Poisson likelihood.
 
         With x* the mode, Q_c = Q_prior + A^T diag(d) A, d = e exp(A x*),
@@ -946,20 +1041,22 @@ class SpatioTemporalModel:
         unconverged x*, so the gradient matches the objective as evaluated."""
         import torch
 
-        thetas = [np.asarray(t, dtype=np.float64) for t in thetas]
+        thetas, precision = tok["thetas"], tok["precision"]
         K = len(thetas)
         n, b = self.nt, self.ns
         s = self._stream()
-        sls = [self.slot(j) for j in range(K)]
-        for sl in sls[1:]:
-            sl.x.copy_(sls[0].x)  # warm start every point from the current mode
-        _lib.check(self.lib.bta_reset_status(self.h.bind_stream()), "reset")
-        self._newton(sls, thetas)
+        sls = self.slots[:K]
         for sl in sls:
             if sl.Sc is None:
                 sl.Sc = BTAMatrix(n, b, self.nb, self._dev)
             sl.Sc.buf.copy_(sl.Qc.buf)
-        self.selinv_batched([sl.Sc for sl in sls] + [sl.Qp for sl in sls], precision)
+        # inverses of Q_c's diagonal factor blocks at the mode: the selected
+        # inversion of its copy and the two sweeps of the z solve share them
+        use_v = self._inverses_fit(sls)
+        Vc = [self._slot_inverses(sl) for sl in sls] if use_v else [None] * K
+        if use_v:
+            self.block_inverses([sl.Qc for sl in sls], Vc)
+        self.selinv_batched([sl.Sc for sl in sls] + [sl.Qp for sl in sls], precision, Vc + [None] * K)
         for sl in sls:
             self._check(self.lib.bta_obs_quad(s, self.nobs, _lib.ptr(self.obs_off), _lib.ptr(self.obs_dst),
                                               _lib.ptr(self.obs_w), _lib.ptr(sl.Sc.buf), self.nb, _lib.ptr(self.X),
@@ -967,8 +1064,12 @@ class SpatioTemporalModel:
                                               _lib.ptr(sl.hvec)), "obs_quad")
             self.spmv(self.AT_rowptr, self.AT_col, self.AT_val, self.N, sl.hvec, sl.z)
             self.dot_to(sl.hvec, self.ones_obs, sl.scal[7:8])  # <S_c, A^T diag(d) A>
-        self.sweep_batched([sl.Qc for sl in sls], [sl.z for sl in sls], 0)
-        self.sweep_batched([sl.Qc for sl in sls], [sl.z for sl in sls], 1)
+        if use_v:
+            self.sweep_inv_batched([sl.Qc for sl in sls], Vc, [sl.z for sl in sls], 0)
+            self.sweep_inv_batched([sl.Qc for sl in sls], Vc, [sl.z for sl in sls], 1)
+        else:
+            self.sweep_batched([sl.Qc for sl in sls], [sl.z for sl in sls], 0)
+            self.sweep_batched([sl.Qc for sl in sls], [sl.z for sl in sls], 1)
         for sl in sls:
             self._check(self.lib.bta_axpby(s, self.N, 1.0, _lib.ptr(sl.upd), -0.5, _lib.ptr(sl.z)), "axpby")
             args = (s, n, b, _lib.ptr(self.u_rowptr), _lib.ptr(self.u_col), _lib.ptr(self.u_vals4))
@@ -998,6 +1099,114 @@ class SpatioTemporalModel:
             tip = self.fe_prec * float(torch.trace(sl.Sc.T).item()) if self.nb else 0.0
             rc, rp = self._identity_residuals(theta, Ic, Ip, rest, tip)
             self.last_check.append({"precision": precision, "residual_c": rc, "residual_p": rp, "fallback": False})
-            fs.append(self._f_poisson(sl, theta))
             grads.append(grad)
+        fs = list(tok["fs"])
         return self._mixed_fallback(thetas, fs, grads, precision)
+
+
+# ------------------------------------------------------------------ groups
+# The Gaussian adjoint of several models at once: every launch of the forward
+# (factorisations, block inverses, sweeps) and of the backward (selected
+# inversions) takes the matrices of all models together, so instances of
+# different block sizes -- e.g. bivariate and univariate models -- share the
+# launches.  A group with one model is the ordinary batched evaluation.
+
+def _gauss_forward_group(jobs, factor_precision="fp64"):
+    """jobs: [(model, thetas)] with Gaussian likelihoods on one device;
+    factor_precision: arithmetic of the factorisations' Schur updates."""
+    lead = jobs[0][0]
+    parts = []
+    _lib.check(lead.lib.bta_reset_status(lead.h.bind_stream()), "reset")
+    for m, thetas in jobs:
+        sls = [m.slot(j) for j in range(len(thetas))]
+        for sl, th in zip(sls, thetas):
+            m._gauss_conditional(th, sl)
+            m.assemble_prior_bt(th, sl)
+        parts.append((m, sls, thetas))
+    Qc = [sl.Qc for _, sls, _ in parts for sl in sls]
+    Qp = [sl.Qp for _, sls, _ in parts for sl in sls]
+    lead.factor_batched(Qc + Qp, factor_precision)
+    # inverses of Q_c's diagonal factor blocks: the sweeps become n dependent
+    # matrix-vector steps, and the selected inversion reuses them
+    Vc = [m._slot_inverses(sl) for m, sls, _ in parts for sl in sls]
+    lead.block_inverses(Qc, Vc)
+    xs = []
+    for m, sls, thetas in parts:
+        for sl, th in zip(sls, thetas):
+            m.logdet_to(sl.Qc, sl.scal[0:1])
+            m.logdet_to(sl.Qp, sl.scal[2:3])
+            m._gauss_rhs(th, sl)
+            sl.x.copy_(sl.rhs)
+            xs.append(sl.x)
+    lead.sweep_inv_batched(Qc, Vc, xs, 0)
+    for m, sls, _ in parts:
+        for sl in sls:
+            m.dot_to(sl.x, sl.x, sl.scal[1:2])  # b^T Q^-1 b = |L^-1 b|^2
+    lead.sweep_inv_batched(Qc, Vc, xs, 1)  # mu
+    return parts
+
+
+def _gauss_backward_group(jobs):
+    """jobs: [(model, token)] whose forwards ran together (or alone) and are
+    still on the device, all with the same precision; returns [(fs, grads)]."""
+    lead = jobs[0][0]
+    precision = jobs[0][1]["precision"]
+    mats, Vs = [], []
+    for m, tok in jobs:
+        K = len(tok["thetas"])
+        n, ns, nv = m.nt, m.ns, m.nv
+        stream = m._stream()
+        pat = (_lib.ptr(m.u_rowptr), _lib.ptr(m.u_col), _lib.ptr(m.u_vals4))
+        for sl in m.slots[:K]:
+            # per variate |A_v mu|^2 and (A_v mu)^T y_v; mu^T (E_tt' (x) K) mu per sub-block
+            m.spmv(m.A_rowptr, m.A_col, m.A_val, m.nobs, sl.x, sl.eta)
+            for j, (lo, hi) in enumerate(m.var_ranges):
+                m.dot_to(sl.eta[lo:hi], sl.eta[lo:hi], sl.vscal[3 * j + 1:3 * j + 2])
+                m.dot_to(sl.eta[lo:hi], m.y[lo:hi], sl.vscal[3 * j + 2:3 * j + 3])
+            m._check(m.lib.bta_block_quad_mv(stream, n, ns, nv, *pat, _lib.ptr(sl.x), _lib.ptr(sl.quad_st)),
+                     "block_quad")
+        mats += [sl.Qc for sl in m.slots[:K]] + [sl.Qp for sl in m.slots[:K]]
+        Vs += [sl.Vc for sl in m.slots[:K]] + [None] * K
+    # selected inverses of every matrix of the group, then their contractions
+    lead.selinv_batched(mats, precision, Vs)
+    for m, tok in jobs:
+        K = len(tok["thetas"])
+        n, ns, nv = m.nt, m.ns, m.nv
+        stream = m._stream()
+        pat = (_lib.ptr(m.u_rowptr), _lib.ptr(m.u_col), _lib.ptr(m.u_vals4))
+        for sl in m.slots[:K]:
+            Dc, Lc, _, _ = sl.Qc.ptrs()
+            Dp, Lp, _, _ = sl.Qp.ptrs()
+            for (Dm, Lm, out) in ((Dc, Lc, sl.inner_c), (Dp, Lp, sl.inner_p)):
+                m._check(m.lib.bta_block_inner_mv(stream, n, ns, nv, *pat, Dm, Lm, _lib.ptr(out)), "block_inner")
+            for j in range(len(m.var_ranges)):
+                m._check(m.lib.bta_gather_dot(stream, m.nent, _lib.ptr(m.ent_dst), _lib.ptr(m.ata_w_var[j]),
+                                              _lib.ptr(sl.Qc.buf), _lib.ptr(m.part), m.nparts,
+                                              _lib.ptr(sl.vscal[3 * j:3 * j + 1])), "gather_dot")
+    lead.status()
+    return [m._gauss_gradients(tok["thetas"], precision) for m, tok in jobs]
+
+
+def adjoint_group(jobs, precision="fp64"):
+    """(f, exact gradient) of several Gaussian models at once:
+    jobs = [(model, thetas)], each model on the same device with its own
+    points.  All factorisations, block inverses, sweeps and selected
+    inversions of every model's Q_c and Q_prior share their launches (the
+    instances may have different block and arrowhead sizes).  Returns
+    [(fs, grads)] per job; the per-point accuracy check and FP64 fallback
+    of each model apply as in ``objective_adjoint_batched``."""
+    if precision not in _PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
+    jobs = [(m, [np.asarray(t, dtype=np.float64) for t in ths]) for m, ths in jobs]
+    if any(not m.gaussian for m, _ in jobs):
+        raise NotImplementedError("grouped adjoint evaluation: Gaussian likelihoods")
+    if len({id(m) for m, _ in jobs}) != len(jobs):
+        raise ValueError("each model may appear once in a group")
+    fp = jobs[0][0].factor_precision if precision != "fp64" else "fp64"
+    _gauss_forward_group(jobs, fp)
+    toks = []
+    for m, thetas in jobs:
+        m._fwd_gen = getattr(m, "_fwd_gen", 0) + 1
+        m._fwd_token = None  # consumed by the backward below
+        toks.append((m, {"gen": m._fwd_gen, "thetas": thetas, "precision": precision, "fs": None}))
+    return _gauss_backward_group(toks)

@@ -320,6 +320,8 @@ CONFIGS = {
     "pst_2500x60": dict(ns=2500, nt=60, nb=6, no=800, theta=(-1.2, 0.8, -0.3), likelihood="poisson",
                         log_intensity_scale=0.4),
     "gst_4000x250": dict(ns=4000, nt=250, nb=6, no=1500, theta=(-1.0, 1.0, 0.0, 2.0), likelihood="gaussian"),
+    # the univariate members of the mixed-size batch (blocks 600 x 600, one fixed effect)
+    "gst_600x40": dict(ns=600, nt=40, nb=1, no=200, theta=(-1.0, 1.0, 0.0, 2.0), likelihood="gaussian"),
 }
 
 
@@ -330,6 +332,14 @@ COREG_CONFIGS = {
                                      0.0, 0.2, -0.1, 0.5, -0.3, 0.4)),
     "gst_coreg2_600x40": dict(ns=600, nt=40, nv=2, nb=1, no=200,
                               theta=(-1.0, 1.0, 2.0, -0.8, 0.9, 1.8, 0.0, 0.2, 0.5)),
+}
+
+
+# A batch of instances of uneven block sizes evaluated in shared launches:
+# (workload, theta points) per member -- 8 bivariate (blocks 1200 x 1200) and
+# 16 univariate (600 x 600) points on the same mesh size.
+MIXED_BATCHES = {
+    "mixed_8x1200_16x600": [("gst_coreg2_600x40", 8), ("gst_600x40", 16)],
 }
 
 

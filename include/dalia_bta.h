@@ -98,15 +98,31 @@ int bta_pobtasi_batched_ex(bta_handle_t h, int count, const int64_t* n, const in
                            int precision);
 
 /*
+ * The batched factorisation with the previous block column's Schur update
+ * (D_i -= L_{i-1} L_{i-1}^T, Ab_i -= Ab_{i-1} L_{i-1}^T) in the given
+ * BTA_PREC_* arithmetic: with BTA_PREC_I8SLICE or BTA_PREC_TF32X3 it runs as
+ * one grouped tensor-core GEMM per block column between the panel launches,
+ * while the diagonal-block POTRF, the triangular solves inside the panel,
+ * the arrow tip and every stored block stay FP64.  BTA_PREC_FP64 is
+ * bta_pobtaf_batched.  No counterpart in the reference (Serinv computes in
+ * the precision of its arrays).
+ */
+int bta_pobtaf_batched_ex(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                          double* const* D, double* const* L, double* const* Ab, double* const* T, int64_t* info,
+                          int precision);
+
+/*
  * Inverses of the diagonal factor blocks, V[k][i] = L_ii^-1 (n[k] blocks of
  * b[k] x b[k], lower triangular, zeros above the diagonal) into caller
  * buffers; with them a triangular sweep is n dependent steps of two
  * bandwidth-bound matrix-vector products (bta_pobtas_inv_batched: same
  * trans and rhs conventions as bta_pobtas_batched; D is not read), and the
  * selected inversion skips its own block inversion
- * (bta_pobtasi_batched_v; V == NULL computes them as bta_pobtasi_batched_ex
- * does).  No counterpart in the reference: Serinv's pobtas solves with the
- * factor blocks directly.
+ * (bta_pobtasi_batched_v; V == NULL, or V[k] == NULL for one instance,
+ * computes them as bta_pobtasi_batched_ex does: chunk by chunk as the
+ * recurrence reaches them, in at most 512 MiB of workspace per instance).
+ * No counterpart in the reference: Serinv's pobtas solves with the factor
+ * blocks directly.
  */
 int bta_block_inverses(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const double* const* D,
                        double* const* V);
@@ -244,6 +260,27 @@ int bta_prof_read(double* ms, long long* counts);
  * needs no device.  BTA_ERR_INVALID when cap is too small.
  */
 int bta_panel_task_list(int count, const int* b, const int* a, const int* flags, int* out, int cap, int* n_out);
+/* The same with the queue lookahead the autotuner may choose (tile columns by
+ * which the previous-column terms run ahead; bta_panel_task_list uses 2). */
+int bta_panel_task_list_ex(int count, const int* b, const int* a, const int* flags, int lookahead, int* out, int cap,
+                           int* n_out);
+
+/*
+ * Autotuner (no counterpart in the reference).  Launch configurations of the
+ * factorisation's block-column kernel (queue lookahead, resident CTAs per SM)
+ * and of the persistent sweep (CTAs per SM, row segments) are tuned online:
+ * the first launches of a new launch shape try every candidate (twice for
+ * the factorisation's block columns, once for a sweep) on the real work,
+ * timed by CUDA events, and the fastest is kept for that shape on that
+ * device.  DALIA_B200_TUNE=0 turns it off; DALIA_B200_TUNE_CACHE=<file>
+ * reads earlier decisions from, and appends new ones to, that file.
+ * bta_tune_report writes one line per decision ("family|device|shape
+ * best=<candidate> ms=<time of each candidate>") into buf (cap bytes, NUL
+ * terminated) and its full length to *len; BTA_ERR_INVALID when truncated.
+ */
+int bta_tune_report(char* buf, size_t cap, size_t* len);
+/* Launch shapes whose candidates are still being tried. */
+int bta_tune_pending(void);
 
 #ifdef __cplusplus
 }

@@ -45,16 +45,25 @@ class Inst:
         return bool(self.flags & HAS_ABPREV) and self.a > 0
 
 
-def task_list(insts):
+# queue lookaheads the autotuner chooses from (2 is the default)
+LOOKAHEADS = [1, 2, 4]
+
+
+def task_list(insts, lookahead=None):
     lib = _lib.load()
     k = len(insts)
     b = (ctypes.c_int * k)(*[i.b for i in insts])
     a = (ctypes.c_int * k)(*[i.a for i in insts])
     f = (ctypes.c_int * k)(*[i.flags for i in insts])
     n = ctypes.c_int(0)
-    assert lib.bta_panel_task_list(k, b, a, f, None, 0, ctypes.byref(n)) == _lib.BTA_ERR_INVALID
+    if lookahead is None:
+        call = lambda out, cap: lib.bta_panel_task_list(k, b, a, f, out, cap, ctypes.byref(n))  # noqa: E731
+    else:
+        call = lambda out, cap: lib.bta_panel_task_list_ex(k, b, a, f, lookahead, out, cap,  # noqa: E731
+                                                            ctypes.byref(n))
+    assert call(None, 0) == _lib.BTA_ERR_INVALID
     out = (ctypes.c_int * (4 * n.value))()
-    assert lib.bta_panel_task_list(k, b, a, f, out, n.value, ctypes.byref(n)) == _lib.BTA_OK
+    assert call(out, n.value) == _lib.BTA_OK
     return [tuple(out[4 * i:4 * i + 4]) for i in range(n.value)]
 
 
@@ -90,10 +99,11 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("look", LOOKAHEADS)
 @pytest.mark.parametrize("ci", range(len(CASES)))
-def test_queue_covers_every_tile_once(ci):
+def test_queue_covers_every_tile_once(ci, look):
     insts = CASES[ci]
-    tasks = task_list(insts)
+    tasks = task_list(insts, look)
     pos = {}
     for i, (m, kind, p, r) in enumerate(tasks):
         key = (m, "prev" if kind == PREV else ("tip" if kind == TIP else "tile"), p, r)
@@ -117,13 +127,14 @@ def test_queue_covers_every_tile_once(ci):
     assert len(tasks) == n_tiles + n_prev + sum(inst.tip for inst in insts)
 
 
+@pytest.mark.parametrize("look", LOOKAHEADS)
 @pytest.mark.parametrize("ci", range(len(CASES)))
-def test_queue_is_topological(ci):
+def test_queue_is_topological(ci, look):
     """Inputs of every task are produced earlier in the queue, directly or
     through the chain (whose step q consumes the tasks of tiles (q, q-1) and
     (q, q))."""
     insts = CASES[ci]
-    tasks = task_list(insts)
+    tasks = task_list(insts, look)
     where = {}
     for i, (m, kind, p, r) in enumerate(tasks):
         out = produces(kind, p, r)
@@ -193,12 +204,18 @@ def simulate(insts, tasks, workers):
             return finished
 
 
+@pytest.mark.parametrize("look", LOOKAHEADS)
 @pytest.mark.parametrize("ci", range(len(CASES)))
-@pytest.mark.parametrize("workers", [1, 2, 3, 7, 40, 437])
-def test_queue_drains_with_any_number_of_ctas(ci, workers):
+@pytest.mark.parametrize("workers", [1, 2, 3, 7, 40, 148, 296, 437])
+def test_queue_drains_with_any_number_of_ctas(ci, workers, look):
     insts = CASES[ci]
-    tasks = task_list(insts)
+    tasks = task_list(insts, look)
     assert simulate(insts, tasks, workers) == len(tasks)
+
+
+def test_default_lookahead_is_two():
+    for insts in CASES:
+        assert task_list(insts) == task_list(insts, 2)
 
 
 def test_task_list_rejects_bad_arguments():
@@ -208,6 +225,7 @@ def test_task_list_rejects_bad_arguments():
     zero = (ctypes.c_int * 1)(0)
     assert lib.bta_panel_task_list(0, one, zero, zero, None, 0, ctypes.byref(n)) == _lib.BTA_ERR_INVALID
     assert lib.bta_panel_task_list(1, zero, zero, zero, None, 0, ctypes.byref(n)) == _lib.BTA_ERR_INVALID
+    assert lib.bta_panel_task_list_ex(1, one, zero, zero, 0, None, 0, ctypes.byref(n)) == _lib.BTA_ERR_INVALID
 
 
 def noalloc_order(b, a, has_l):
