@@ -93,6 +93,23 @@ int ensure_ws(bta_context* h, size_t bytes) {
 
 inline unsigned long long* info_ptr(bta_context* h) { return reinterpret_cast<unsigned long long*>(h->ctl + 2); }
 
+// Makes the handle's device current for one call and restores the caller's
+// device afterwards: a handle's scratch and launches belong to its device.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(const bta_context* h) {
+    if (!h) return;
+    if (cudaGetDevice(&prev) != cudaSuccess || prev == h->device) {
+      prev = -1;
+      return;
+    }
+    cudaSetDevice(h->device);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
 int cuda_rc(cudaError_t e) { return e == cudaSuccess ? BTA_OK : BTA_ERR_CUDA; }
 int cuda_rc(int e) { return e == 0 ? BTA_OK : BTA_ERR_CUDA; }
 
@@ -299,6 +316,7 @@ int bta_create(bta_handle_t* handle) {
 }
 
 int bta_destroy(bta_handle_t h) {
+  DeviceGuard dg_(h);
   if (!h) return BTA_ERR_INVALID;
   cudaStreamSynchronize(h->stream);
   for (auto& kv : h->tasks) cudaFree(kv.second.first);
@@ -326,6 +344,7 @@ int bta_pobtaf_batched(bta_handle_t h, int count, const int64_t* n, const int64_
 int bta_pobtaf_batched_ex(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
                           double* const* D, double* const* L, double* const* Ab, double* const* T, int64_t* info,
                           int precision) {
+  DeviceGuard dg_(h);
   if (!h || count < 1 || !n || !b || !a || !D) return BTA_ERR_INVALID;
   if (precision != BTA_PREC_FP64 && precision != BTA_PREC_TF32X3 && precision != BTA_PREC_I8SLICE)
     return BTA_ERR_INVALID;
@@ -445,6 +464,7 @@ bool sweep_by_inverses(int count, const int64_t* n, const int64_t* b, const int6
 int bta_pobtas_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
                        const double* const* D, const double* const* L, const double* const* Ab,
                        const double* const* T, double* const* rhs, int trans) {
+  DeviceGuard dg_(h);
   if (!h || count < 1 || count > SWEEP_MAXI || !n || !b || !a || !D || !rhs) return BTA_ERR_INVALID;
   if (trans != 0 && trans != 1) return BTA_ERR_INVALID;
   for (int k = 0; k < count; ++k) {
@@ -590,6 +610,7 @@ inline int64_t inverse_chunk(int64_t n, int64_t b) {
 int bta_pobtasi_batched_v(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
                           double* const* D, double* const* L, double* const* Ab, double* const* T,
                           const double* const* V, int precision) {
+  DeviceGuard dg_(h);
   if (!h || count < 1 || !n || !b || !a || !D) return BTA_ERR_INVALID;
   if (precision != BTA_PREC_FP64 && precision != BTA_PREC_TF32X3 && precision != BTA_PREC_I8SLICE)
     return BTA_ERR_INVALID;
@@ -747,6 +768,7 @@ int bta_panel_task_list_ex(int count, const int* b, const int* a, const int* fla
 
 int bta_block_inverses(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const double* const* D,
                        double* const* V) {
+  DeviceGuard dg_(h);
   if (!h || count < 1 || !n || !b || !D || !V) return BTA_ERR_INVALID;
   size_t need = kAlign;
   for (int k = 0; k < count; ++k) {
@@ -766,6 +788,7 @@ int bta_block_inverses(bta_handle_t h, int count, const int64_t* n, const int64_
 int bta_pobtas_inv_batched(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
                            const double* const* L, const double* const* Ab, const double* const* T,
                            const double* const* V, double* const* rhs, int trans) {
+  DeviceGuard dg_(h);
   if (!h || count < 1 || !n || !b || !a || !V || !rhs || (trans != 0 && trans != 1)) return BTA_ERR_INVALID;
   std::vector<int> ni(count), bi(count), ai(count);
   std::vector<const double*> Lk(count), Abk(count), Tk(count);
@@ -794,6 +817,7 @@ int bta_pobtas_inv_batched(bta_handle_t h, int count, const int64_t* n, const in
 int bta_gemm(bta_handle_t h, int precision, int64_t M, int64_t N, int64_t K, double alpha, const double* A,
              int64_t lda, int a_trans, const double* B, int64_t ldb, int b_kn, double beta, double* C, int64_t ldc,
              int lower_only, int mirror) {
+  DeviceGuard dg_(h);
   if (!h || M < 0 || N < 0 || K < 0 || M > INT32_MAX || N > INT32_MAX || K > INT32_MAX) return BTA_ERR_INVALID;
   if (precision != BTA_PREC_FP64 && precision != BTA_PREC_TF32X3 && precision != BTA_PREC_I8SLICE)
     return BTA_ERR_INVALID;
@@ -808,6 +832,7 @@ int bta_gemm(bta_handle_t h, int precision, int64_t M, int64_t N, int64_t K, dou
 
 int bta_logdet(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D, const double* T, int include_tip,
                double* out_device, double* out_host) {
+  DeviceGuard dg_(h);
   if (!h || n < 1 || b < 1 || a < 0 || !D || (include_tip && a > 0 && !T)) return BTA_ERR_INVALID;
   int rc = ensure_ws(h, align_up((size_t)(n + 2) * 8));
   if (rc) return rc;
@@ -824,11 +849,13 @@ int bta_logdet(bta_handle_t h, int64_t n, int64_t b, int64_t a, const double* D,
 }
 
 int bta_get_status(bta_handle_t h, int64_t* info) {
+  DeviceGuard dg_(h);
   if (!h) return BTA_ERR_INVALID;
   return check_status(h, info);
 }
 
 int bta_reset_status(bta_handle_t h) {
+  DeviceGuard dg_(h);
   if (!h) return BTA_ERR_INVALID;
   return reset_status(h);
 }
@@ -836,6 +863,7 @@ int bta_reset_status(bta_handle_t h) {
 int bta_gather_coo(bta_handle_t h, int64_t n, int64_t b, int64_t a, const int64_t* row, const int64_t* col,
                    int64_t nnz, int sparsity_bt, const double* D, const double* L, const double* Ab, const double* T,
                    double* out) {
+  DeviceGuard dg_(h);
   if (!h || n < 1 || b < 1 || a < 0 || !D || (n > 1 && !L) || nnz < 0 || (nnz > 0 && !out)) return BTA_ERR_INVALID;
   if (!sparsity_bt && a > 0 && (!Ab || !T)) return BTA_ERR_INVALID;
   if (nnz > 0) {
@@ -850,6 +878,7 @@ int bta_gather_coo(bta_handle_t h, int64_t n, int64_t b, int64_t a, const int64_
 
 int bta_scatter_coo(bta_handle_t h, int64_t n, int64_t b, int64_t a, const int64_t* row, const int64_t* col,
                     const double* val, int64_t nnz, int sparsity_bt, double* D, double* L, double* Ab, double* T) {
+  DeviceGuard dg_(h);
   if (!h || n < 1 || b < 1 || a < 0 || !D || (n > 1 && !L) || nnz < 0) return BTA_ERR_INVALID;
   if (!sparsity_bt && a > 0 && (!Ab || !T)) return BTA_ERR_INVALID;
   cudaStream_t s = h->stream;

@@ -36,25 +36,40 @@
 
 #include "gemm.cuh"
 #include "prof.cuh"
+#include "tune.cuh"
 
 namespace bta {
 namespace {
 
 constexpr int OZ_S = 7;                        // digits per operand
-constexpr int QBM = 128, QBN = 64, QBK = 32;   // output tile, k-slab (32 int8 = one 32-byte row)
+constexpr int QBM = 128, QBK = 32;             // output tile rows, k-slab (32 int8 = one 32-byte row)
 constexpr int IMG = 64 * QBK;                  // one 64-row digit image (2 KB)
 constexpr int QSTAGES = 3;
 constexpr int A_SLICE = 2 * IMG;               // 128 rows
-constexpr int B_SLICE = IMG;                   // 64 rows
-constexpr int QSTAGE_BYTES = OZ_S * (A_SLICE + B_SLICE);
 constexpr int QTHREADS = 6 * 32;               // 4 epilogue warps, producer warp, MMA warp
 constexpr int QSTAGE_LD = 65;                  // epilogue staging: 32 rows x 64 columns per warp, padded
 constexpr int QEPI_BYTES = 4 * 32 * QSTAGE_LD * 8;
-constexpr size_t QSMEM_BYTES = size_t(QSTAGES) * QSTAGE_BYTES + QEPI_BYTES + 256 + 1024;
-constexpr int TMEM_COLS = 512;                 // OZ_S accumulators of QBN columns
+constexpr int TMEM_COLS = 512;
 constexpr long long QWAIT_CYCLES = 4000000000LL;
 constexpr int EXP_NONE = -1100;                // exponent of an all-zero row
-static_assert(OZ_S * QBN <= TMEM_COLS, "accumulators exceed tensor memory");
+
+// The output tile is QBM x BN, BN = 64 or 32 columns (a template parameter
+// of the kernel; the autotuner picks it per launch shape).  The OZ_S level
+// accumulators of a tile take OZ_S BN columns of tensor memory: with BN = 64
+// one set (448 of 512 columns), so a tile's products wait until the epilogue
+// has read the previous tile's; with BN = 32 two sets (224 columns each, at
+// columns 0 and 256), so the products of tile t+1 run while the epilogue
+// drains tile t -- at the price of half the B operand per A slab.
+template <int BN>
+struct QTile {
+  static constexpr int B_SLICE = BN * QBK;                   // BN rows of a digit image
+  static constexpr int STAGE_BYTES = OZ_S * (A_SLICE + B_SLICE);
+  static constexpr int NSETS = BN == 32 ? 2 : 1;             // accumulator sets in tensor memory
+  static constexpr int SET_COLS = 256;
+  static constexpr size_t SMEM_BYTES = size_t(QSTAGES) * STAGE_BYTES + QEPI_BYTES + 256 + 1024;
+  static_assert(BN == 32 || BN == 64, "tile width");
+  static_assert(OZ_S * BN <= (NSETS == 2 ? SET_COLS : TMEM_COLS), "accumulators exceed tensor memory");
+};
 
 // Instruction descriptor: D S32 (bits 4-5 = 2), A and B signed 8-bit (bits
 // 7-9, 10-12 = 1), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
@@ -406,21 +421,25 @@ struct QBatch {
   QProb p[QMAXP];
 };
 
-// lower-only tiles: (tm, tn) with tn * QBN <= tm * QBM + QBM - 1
-__device__ __forceinline__ int lower_tiles_row(int tm, int tnn) { return min(2 * tm + 2, tnn); }
+// lower-only tiles: (tm, tn) with tn * BN <= tm * QBM + QBM - 1
+__host__ __device__ __forceinline__ int lower_tiles_row(int tm, int tnn, int bn) {
+  return min((tm + 1) * (QBM / bn), tnn);
+}
 
+template <int BN>
 __device__ __forceinline__ int qseg_range(const QSeg& s, int m0, int n0, int& kt0) {
   int kmin = 0, kmax = s.K;
   if (s.kflags & GF_K_GE_M) kmin = max(kmin, m0);
   if (s.kflags & GF_K_GE_N) kmin = max(kmin, n0);
   if (s.kflags & GF_K_LE_M) kmax = min(kmax, m0 + QBM);
-  if (s.kflags & GF_K_LE_N) kmax = min(kmax, n0 + QBN);
+  if (s.kflags & GF_K_LE_N) kmax = min(kmax, n0 + BN);
   kt0 = kmin / QBK;
   const int kt1 = (kmax + QBK - 1) / QBK;
   return kt1 > kt0 ? kt1 - kt0 : 0;
 }
 
 // Tile t of a batch: problem, tile row, tile column.
+template <int BN>
 __device__ __forceinline__ void decode_tile(const QBatch& batch, int t, int& pi, int& tm, int& tn) {
   pi = 0;
   while (pi + 1 < batch.count && t >= batch.tile_start[pi + 1]) ++pi;
@@ -428,7 +447,7 @@ __device__ __forceinline__ void decode_tile(const QBatch& batch, int t, int& pi,
   int local = t - batch.tile_start[pi];
   tm = 0;
   if (P.cflags & GC_LOWER) {
-    while (local >= lower_tiles_row(tm, P.tnn)) local -= lower_tiles_row(tm++, P.tnn);
+    while (local >= lower_tiles_row(tm, P.tnn, BN)) local -= lower_tiles_row(tm++, P.tnn, BN);
     tn = local;
   } else {
     tm = local / P.tnn;
@@ -436,28 +455,34 @@ __device__ __forceinline__ void decode_tile(const QBatch& batch, int t, int& pi,
   }
 }
 
+template <int BN>
 __device__ __forceinline__ int tile_steps(const QProb& P, int m0, int n0) {
   int nsteps = 0;
   for (int si = 0; si < P.nseg; ++si) {
     int kt0;
-    nsteps += qseg_range(P.seg[si], m0, n0, kt0);
+    nsteps += qseg_range<BN>(P.seg[si], m0, n0, kt0);
   }
   return nsteps;
 }
 
 // Persistent: CTA c takes tiles c, c + grid, ...  The producer's ring runs
-// across tile boundaries; the MMA warp starts a tile once the epilogue has
-// read the previous tile's accumulators out of tensor memory (tmem_empty), so
-// the epilogue's scaling and stores overlap the next tile's products.
+// across tile boundaries; tile number it (of this CTA) accumulates into set
+// it % NSETS, and the MMA warp starts it once the epilogue has read the
+// accumulators of tile it - NSETS out of tensor memory (tmem_empty of that
+// set), so the epilogue's scaling and stores overlap later tiles' products.
+template <int BN>
 __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_constant__ QBatch batch, int total_tiles,
                                                                int* abort_flag) {
+  using TT = QTile<BN>;
+  constexpr int NSETS = TT::NSETS;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
-  double* epi_stage = reinterpret_cast<double*>(smem + QSTAGES * QSTAGE_BYTES);
-  uint8_t* bars = smem + QSTAGES * QSTAGE_BYTES + QEPI_BYTES;
-  const uint32_t full0 = smem_u32(bars), empty0 = full0 + 8 * QSTAGES, done_bar = empty0 + 8 * QSTAGES;
-  const uint32_t tmem_empty = done_bar + 8, drain_bar = done_bar + 16;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 8 * (2 * QSTAGES + 3));
+  double* epi_stage = reinterpret_cast<double*>(smem + QSTAGES * TT::STAGE_BYTES);
+  uint8_t* bars = smem + QSTAGES * TT::STAGE_BYTES + QEPI_BYTES;
+  // barriers: full[QSTAGES], empty[QSTAGES], done[2], tmem_empty[2], drain
+  const uint32_t full0 = smem_u32(bars), empty0 = full0 + 8 * QSTAGES, done0 = empty0 + 8 * QSTAGES;
+  const uint32_t tmem_empty0 = done0 + 16, drain_bar = done0 + 32;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 8 * (2 * QSTAGES + 5));
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
@@ -472,8 +497,10 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
       mbar_init(full0 + 8 * s, 1);
       mbar_init(empty0 + 8 * s, 1);
     }
-    mbar_init(done_bar, 1);
-    mbar_init(tmem_empty, 4);  // one arrival per epilogue warp
+    for (int k = 0; k < 2; ++k) {
+      mbar_init(done0 + 8 * k, 1);
+      mbar_init(tmem_empty0 + 8 * k, 4);  // one arrival per epilogue warp
+    }
     mbar_init(drain_bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -490,12 +517,15 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
       bool ok = true;
       for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
         int pi, tm, tn;
-        decode_tile(batch, t, pi, tm, tn);
+        decode_tile<BN>(batch, t, pi, tm, tn);
         const QProb& P = batch.p[pi];
+        // B rows of this tile: image (tn BN) / 64, from row (tn BN) % 64 (the
+        // second 32 rows of an image start 1 KB in: four whole 8-row groups)
+        const size_t bimg = (size_t)(tn * BN) / 64, boff = (size_t)((tn * BN) % 64) * QBK;
         for (int si = 0; si < P.nseg && ok; ++si) {
           const QSeg& sg = P.seg[si];
           int kt0;
-          const int nk = qseg_range(sg, tm * QBM, tn * QBN, kt0);
+          const int nk = qseg_range<BN>(sg, tm * QBM, tn * BN, kt0);
           for (int i = 0; i < nk; ++i, ++step) {
             const int st = step % QSTAGES;
             if (step >= QSTAGES && !mbar_wait(empty0 + 8 * st, ((step / QSTAGES) - 1) & 1, abort_flag)) {
@@ -504,13 +534,13 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
             }
             const int kt = kt0 + i;
             const uint32_t bar = full0 + 8 * st;
-            mbar_expect_tx(bar, QSTAGE_BYTES);
-            const uint32_t dst = stage0 + st * QSTAGE_BYTES;
+            mbar_expect_tx(bar, TT::STAGE_BYTES);
+            const uint32_t dst = stage0 + st * TT::STAGE_BYTES;
 #pragma unroll
             for (int p = 0; p < OZ_S; ++p) {
               bulk_g2s(dst + p * A_SLICE, sg.A + (((size_t)p * sg.KT + kt) * sg.RBa + 2 * tm) * IMG, A_SLICE, bar);
-              bulk_g2s(dst + OZ_S * A_SLICE + p * B_SLICE, sg.B + (((size_t)p * sg.KT + kt) * sg.RBb + tn) * IMG,
-                       B_SLICE, bar);
+              bulk_g2s(dst + OZ_S * A_SLICE + p * TT::B_SLICE,
+                       sg.B + (((size_t)p * sg.KT + kt) * sg.RBb + bimg) * IMG + boff, TT::B_SLICE, bar);
             }
           }
         }
@@ -523,10 +553,12 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
       bool ok = true;
       for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x, ++it) {
         int pi, tm, tn;
-        decode_tile(batch, t, pi, tm, tn);
-        const int nsteps = tile_steps(batch.p[pi], tm * QBM, tn * QBN);
-        // the epilogue has read the previous tile's accumulators
-        if (it > 0 && !mbar_wait(tmem_empty, (it - 1) & 1, abort_flag)) break;
+        decode_tile<BN>(batch, t, pi, tm, tn);
+        const int nsteps = tile_steps<BN>(batch.p[pi], tm * QBM, tn * BN);
+        const int set = it % NSETS, use = it / NSETS;
+        const uint32_t tacc = tmem + (uint32_t)(set * TT::SET_COLS);
+        // the epilogue has read the accumulators of this set's previous tile
+        if (use > 0 && !mbar_wait(tmem_empty0 + 8 * set, (use - 1) & 1, abort_flag)) break;
         tc_fence_after();
         for (int ks = 0; ks < nsteps; ++ks, ++step) {
           const int st = step % QSTAGES;
@@ -535,26 +567,26 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
             break;
           }
           tc_fence_after();
-          const uint32_t a0 = stage0 + st * QSTAGE_BYTES, b0 = a0 + OZ_S * A_SLICE;
+          const uint32_t a0 = stage0 + st * TT::STAGE_BYTES, b0 = a0 + OZ_S * A_SLICE;
 #pragma unroll
           for (int p = 0; p < OZ_S; ++p) {
-            // digit p of A against the stacked digit images q = q0 .. q0+nq-1
-            // of B (consecutive 64-row images form one K-major operand of
-            // 64 nq rows): product (p, q) lands in columns (p + q) QBN .. of
-            // tensor memory, the accumulator of d = p + q.  The first
-            // products of a tile, p = 0 at its first step, overwrite every
-            // accumulator.
+            // digit p of A against the stacked digit slices q = q0 .. q0+nq-1
+            // of B (consecutive BN-row slices form one K-major operand of
+            // BN nq rows): product (p, q) lands in columns (p + q) BN .. of
+            // the set's tensor memory, the accumulator of d = p + q.  The
+            // first products of a tile, p = 0 at its first step, overwrite
+            // every accumulator.
             const uint32_t acc = (ks > 0 || p > 0) ? 1u : 0u;
 #pragma unroll
-            for (int q0 = 0; q0 < OZ_S - p; q0 += QMMA_NMAX / QBN) {
-              const int nq = min(QMMA_NMAX / QBN, OZ_S - p - q0);
-              mma_i8(tmem + (uint32_t)((p + q0) * QBN), sw32_desc(a0 + p * A_SLICE), sw32_desc(b0 + q0 * B_SLICE),
-                     idesc_i8(nq * QBN), acc);
+            for (int q0 = 0; q0 < OZ_S - p; q0 += QMMA_NMAX / BN) {
+              const int nq = min(QMMA_NMAX / BN, OZ_S - p - q0);
+              mma_i8(tacc + (uint32_t)((p + q0) * BN), sw32_desc(a0 + p * A_SLICE),
+                     sw32_desc(b0 + q0 * TT::B_SLICE), idesc_i8(nq * BN), acc);
             }
           }
           tc_commit(empty0 + 8 * st);
         }
-        tc_commit(done_bar);  // also for a tile without products: the epilogue then writes beta C
+        tc_commit(done0 + 8 * set);  // also for a tile without products: the epilogue then writes beta C
       }
       // every product issued has completed before the tensor memory is freed
       tc_commit(drain_bar);
@@ -572,18 +604,19 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
     int it = 0;
     for (int t = blockIdx.x; t < total_tiles; t += gridDim.x, ++it) {
       int pi, tm, tn;
-      decode_tile(batch, t, pi, tm, tn);
+      decode_tile<BN>(batch, t, pi, tm, tn);
       const QProb& P = batch.p[pi];
-      const int m0 = tm * QBM, n0 = tn * QBN;
-      const int nsteps = tile_steps(P, m0, n0);
-      if (!__all_sync(0xffffffffu, mbar_wait(done_bar, it & 1, abort_flag))) break;
+      const int m0 = tm * QBM, n0 = tn * BN;
+      const int nsteps = tile_steps<BN>(P, m0, n0);
+      const int set = it % NSETS, use = it / NSETS;
+      if (!__all_sync(0xffffffffu, mbar_wait(done0 + 8 * set, use & 1, abort_flag))) break;
       tc_fence_after();
       const bool have = nsteps > 0;
       const int row = m0 + 32 * warp + lane;
       const bool rowok = row < P.M;
       const int er = rowok ? max(P.eA[row], EXP_NONE) : 0;
 #pragma unroll 1
-      for (int c = 0; c < QBN / 32; ++c) {
+      for (int c = 0; c < BN / 32; ++c) {
         const int col0 = n0 + 32 * c;
         const int fcol = (col0 + lane < P.N) ? max(P.fB[col0 + lane], EXP_NONE) : 0;
         // exponents in the normal range (every tile of ordinary data): two
@@ -598,7 +631,7 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
           for (int j = 0; j < 16; ++j) hi[j] = lo[j] = 0;
           if (have) {
             uint32_t ra[16], rb[16];
-            const uint32_t tcol = trow + (uint32_t)(32 * c + 16 * h);
+            const uint32_t tcol = trow + (uint32_t)(set * TT::SET_COLS + 32 * c + 16 * h);
             tmem_ld16(tcol, ra);
 #pragma unroll
             for (int d = 0; d < OZ_S; ++d) {
@@ -613,8 +646,8 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
                 for (int j = 0; j < 16; ++j) cur[j] = ra[j];
               }
               if (d + 1 < OZ_S) {
-                if (d & 1) tmem_ld16(tcol + (uint32_t)((d + 1) * QBN), ra);
-                else tmem_ld16(tcol + (uint32_t)((d + 1) * QBN), rb);
+                if (d & 1) tmem_ld16(tcol + (uint32_t)((d + 1) * BN), ra);
+                else tmem_ld16(tcol + (uint32_t)((d + 1) * BN), rb);
               }
 #pragma unroll
               for (int j = 0; j < 16; ++j) {
@@ -643,13 +676,13 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
       // accumulators read: the next tile's products may start
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(tmem_empty);
+      if (lane == 0) mbar_arrive(tmem_empty0 + 8 * set);
       const bool lower = P.cflags & GC_LOWER;
       const bool mirror = P.cflags & GC_MIRROR;
       double* C = P.C;
       const int rbase = m0 + 32 * warp;
 #pragma unroll 1
-      for (int c = 0; c < QBN / 32; ++c) {
+      for (int c = 0; c < BN / 32; ++c) {
         // row segments: lane = column
         const int col = n0 + 32 * c + lane;
 #pragma unroll 4
@@ -703,7 +736,7 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
     need += align256((size_t)p.M * 4) + align256((size_t)p.N * 4);
     for (int s = 0; s < p.nseg; ++s) {
       const size_t KT = (size_t)(p.seg[s].K + QBK - 1) / QBK;
-      const size_t RBa = 2 * (size_t)((p.M + QBM - 1) / QBM), RBb = (size_t)(p.N + QBN - 1) / QBN;
+      const size_t RBa = 2 * (size_t)((p.M + QBM - 1) / QBM), RBb = (size_t)(p.N + 63) / 64;
       need += align256(OZ_S * KT * RBa * IMG) + align256(OZ_S * KT * RBb * IMG);
       if (p.seg[s].K > 19000) return cudaErrorInvalidValue;  // INT32 accumulation bound
     }
@@ -711,8 +744,19 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
   if (ws_needed) *ws_needed = need;
   if (!ws) return cudaSuccess;
   if (ws_bytes < need || !abort_flag) return cudaErrorInvalidValue;
+  // output tile width: 64 (one accumulator set) or 32 (two sets), chosen by
+  // the autotuner per launch shape
+  long long work = 0;
+  for (const GemmProb& p : probs)
+    for (int s = 0; s < p.nseg; ++s) work += (long long)p.M * p.N / 64 * ((p.seg[s].K + 63) / 64);
+  TuneLaunch tl("gemm_i8", {(long long)probs.size(), probs.empty() ? 0 : probs[0].M, probs.empty() ? 0 : probs[0].N,
+                            probs.empty() ? 0 : (long long)probs[0].cflags, work},
+                2, stream);
+  const int BN = tl.choice() == 1 ? 32 : 64;
   {
-    const int e = ensure_smem_attr(reinterpret_cast<const void*>(gemm_i8_kernel), (int)QSMEM_BYTES);
+    const int e = BN == 64
+                      ? ensure_smem_attr(reinterpret_cast<const void*>(gemm_i8_kernel<64>), (int)QTile<64>::SMEM_BYTES)
+                      : ensure_smem_attr(reinterpret_cast<const void*>(gemm_i8_kernel<32>), (int)QTile<32>::SMEM_BYTES);
     if (e != cudaSuccess) return (cudaError_t)e;
   }
   uint8_t* w = static_cast<uint8_t*>(ws);
@@ -729,14 +773,14 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
     q.cflags = p.cflags;
     q.nseg = p.nseg;
     q.tmn = (p.M + QBM - 1) / QBM;
-    q.tnn = (p.N + QBN - 1) / QBN;
+    q.tnn = (p.N + BN - 1) / BN;
     if ((p.cflags & GC_LOWER) && p.M != p.N) return cudaErrorInvalidValue;
     SliceGroup ga{}, gb{};
     ga.rows = p.M;
     ga.RB = 2 * q.tmn;
     ga.nseg = p.nseg;
     gb.rows = p.N;
-    gb.RB = q.tnn;
+    gb.RB = (p.N + 63) / 64;
     gb.nseg = p.nseg;
     for (int s = 0; s < p.nseg; ++s) {
       const GemmSeg& g = p.seg[s];
@@ -805,7 +849,7 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
       const QProb& q = qp[i];
       int tiles = 0;
       if (q.cflags & GC_LOWER) {
-        for (int tm = 0; tm < q.tmn; ++tm) tiles += std::min(2 * tm + 2, q.tnn);
+        for (int tm = 0; tm < q.tmn; ++tm) tiles += lower_tiles_row(tm, q.tnn, BN);
       } else {
         tiles = q.tmn * q.tnn;
       }
@@ -818,7 +862,10 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
     if (total > 0) {
       const int sms = device_sm_count();
       bta::ProfScope _ps(bta::PROF_GEMM, stream);
-      gemm_i8_kernel<<<std::min(total, sms), QTHREADS, QSMEM_BYTES, stream>>>(b, total, abort_flag);
+      if (BN == 64)
+        gemm_i8_kernel<64><<<std::min(total, sms), QTHREADS, QTile<64>::SMEM_BYTES, stream>>>(b, total, abort_flag);
+      else
+        gemm_i8_kernel<32><<<std::min(total, sms), QTHREADS, QTile<32>::SMEM_BYTES, stream>>>(b, total, abort_flag);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

@@ -42,6 +42,21 @@ bool tuning_on() {
   return !(p && std::strcmp(p, "0") == 0);
 }
 
+// DALIA_B200_TUNE_FORCE="family=candidate,..." pins a family's candidate
+// (tests use it to run every variant); -1 when the family is not named.
+int forced(const char* family) {
+  const char* p = std::getenv("DALIA_B200_TUNE_FORCE");
+  if (!p || !*p) return -1;
+  const size_t fl = std::strlen(family);
+  for (const char* q = p; *q;) {
+    if (std::strncmp(q, family, fl) == 0 && q[fl] == '=') return std::atoi(q + fl + 1);
+    const char* c = std::strchr(q, ',');
+    if (!c) break;
+    q = c + 1;
+  }
+  return -1;
+}
+
 // "<device name>/<SM count>" of the current device (cached per device; call
 // with g_mu held)
 std::string device_tag() {
@@ -101,6 +116,11 @@ void save_line(const std::string& key, const Entry& e) {
 
 TuneLaunch::TuneLaunch(const char* family, const std::vector<long long>& key, int ncand, cudaStream_t s, int reps)
     : stream_(s) {
+  const int f = forced(family);
+  if (f >= 0) {
+    choice_ = f < ncand ? f : 0;
+    return;
+  }
   if (ncand <= 1 || !tuning_on()) return;
   std::lock_guard<std::mutex> lk(g_mu);
   std::ostringstream o;

@@ -33,7 +33,9 @@ extern "C" {
 
 typedef struct bta_context* bta_handle_t;
 
-/* Handle life cycle.  The handle binds to the current CUDA device. */
+/* Handle life cycle.  The handle binds to the current CUDA device; every call
+ * on it makes that device current for its duration (the caller's current
+ * device is restored). */
 int bta_create(bta_handle_t* handle);
 int bta_destroy(bta_handle_t handle);
 /* stream: a cudaStream_t (NULL = legacy default stream). */
@@ -272,8 +274,12 @@ int bta_panel_task_list_ex(int count, const int* b, const int* a, const int* fla
  * the first launches of a new launch shape try every candidate (twice for
  * the factorisation's block columns, once for a sweep) on the real work,
  * timed by CUDA events, and the fastest is kept for that shape on that
- * device.  DALIA_B200_TUNE=0 turns it off; DALIA_B200_TUNE_CACHE=<file>
- * reads earlier decisions from, and appends new ones to, that file.
+ * device; the 8-bit-slice GEMM's output tile width (64, or 32 with two
+ * tensor-memory accumulator sets) is chosen the same way per launch shape.
+ * DALIA_B200_TUNE=0 turns it off; DALIA_B200_TUNE_CACHE=<file> reads earlier
+ * decisions from, and appends new ones to, that file;
+ * DALIA_B200_TUNE_FORCE="family=candidate,..." pins candidates (families
+ * "panel", "sweep", "gemm_i8").
  * bta_tune_report writes one line per decision ("family|device|shape
  * best=<candidate> ms=<time of each candidate>") into buf (cap bytes, NUL
  * terminated) and its full length to *len; BTA_ERR_INVALID when truncated.

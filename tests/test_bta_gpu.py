@@ -205,3 +205,106 @@ def test_block_inverse_sweeps_and_selinv(n, b, a):
         assert rel(got[1], ref[1]) < TOL
     if a:
         assert rel(got[2], ref[2]) < TOL and rel(got[3], ref[3]) < TOL
+
+
+class _SerinvSolverCalls:
+    """The calling sequence of DALIA's ``SerinvSolver`` against ``serinv.algs``
+    (``src/dalia/solvers/structured_solver.py:72-190``): the four arrays
+    passed positionally, one sweep per ``pobtas`` call with ``trans="N"``
+    then ``trans="C"`` as keywords, the log-determinant read from the factor's
+    diagonals in place, the selected inversion in place."""
+
+    def __init__(self, algs, D, L, Ab, T):
+        self.algs = algs
+        self.A_diagonal_blocks, self.A_lower_diagonal_blocks = D, L
+        self.A_arrow_bottom_blocks, self.A_arrow_tip_block = Ab, T
+
+    def cholesky(self, sparsity):
+        if sparsity == "bta":
+            self.algs.pobtaf(self.A_diagonal_blocks, self.A_lower_diagonal_blocks, self.A_arrow_bottom_blocks,
+                             self.A_arrow_tip_block)
+        else:
+            self.algs.pobtf(self.A_diagonal_blocks, self.A_lower_diagonal_blocks)
+
+    def solve(self, rhs, sparsity):
+        if sparsity == "bta":
+            for tr in ("N", "C"):
+                self.algs.pobtas(self.A_diagonal_blocks, self.A_lower_diagonal_blocks, self.A_arrow_bottom_blocks,
+                                 self.A_arrow_tip_block, rhs, trans=tr)
+        else:
+            for tr in ("N", "C"):
+                self.algs.pobts(self.A_diagonal_blocks, self.A_lower_diagonal_blocks, rhs, trans=tr)
+        return rhs
+
+    def logdet(self, sparsity, xp):
+        ld = 0.0
+        for i in range(self.A_diagonal_blocks.shape[0]):
+            ld += float(xp.sum(xp.log(xp.diagonal(self.A_diagonal_blocks[i]))))
+        if sparsity == "bta":
+            ld += float(xp.sum(xp.log(xp.diagonal(self.A_arrow_tip_block))))
+        return 2 * ld
+
+    def selected_inversion(self, sparsity):
+        if sparsity == "bta":
+            self.algs.pobtasi(self.A_diagonal_blocks, self.A_lower_diagonal_blocks, self.A_arrow_bottom_blocks,
+                              self.A_arrow_tip_block)
+        else:
+            self.algs.pobtsi(self.A_diagonal_blocks, self.A_lower_diagonal_blocks)
+
+
+@pytest.mark.parametrize("arrays", ["numpy", "torch"])
+@pytest.mark.parametrize("sparsity", ["bta", "bt"])
+def test_serinv_solver_calling_sequence(arrays, sparsity):
+    import torch
+
+    from dalia_b200 import serinv_compat as sc
+
+    n, b, a = 5, 150, 4
+    rng = np.random.default_rng(11)
+    D, L, Ab, T = bta_ref.random_bta(n, b, a, rng)
+    if sparsity == "bt":
+        Ab, T = np.zeros((n, 0, b)), np.zeros((0, 0))
+    M = bta_ref.bta_to_dense(D, L, Ab, T) if a and sparsity == "bta" else bta_ref.bta_to_dense(
+        D, L, np.zeros((n, 0, b)), np.zeros((0, 0)))
+    N = M.shape[0]
+    if arrays == "numpy":
+        arrs, xp = [x.copy() for x in (D, L, Ab, T)], np
+    else:
+        arrs, xp = [torch.from_numpy(x.copy()).cuda() for x in (D, L, Ab, T)], torch
+    solver = _SerinvSolverCalls(sc, *arrs)
+    solver.cholesky(sparsity)
+    assert abs(solver.logdet(sparsity, xp) - np.linalg.slogdet(M)[1]) < 1e-10 * abs(np.linalg.slogdet(M)[1])
+    rhs0 = rng.standard_normal(N)
+    rhs = rhs0.copy() if arrays == "numpy" else torch.from_numpy(rhs0.copy()).cuda()
+    out = solver.solve(rhs, sparsity)
+    assert out is rhs
+    got = out if arrays == "numpy" else out.cpu().numpy()
+    assert rel(got, np.linalg.solve(M, rhs0)) < 1e-10
+    solver.selected_inversion(sparsity)
+    S = np.linalg.inv(M)
+    Dg = arrs[0] if arrays == "numpy" else arrs[0].cpu().numpy()
+    Lg = arrs[1] if arrays == "numpy" else arrs[1].cpu().numpy()
+    for i in range(n):
+        assert rel(Dg[i], S[i * b:(i + 1) * b, i * b:(i + 1) * b]) < 1e-10
+    for i in range(n - 1):
+        assert rel(Lg[i], S[(i + 1) * b:(i + 2) * b, i * b:(i + 1) * b]) < 1e-10
+
+
+def test_handle_on_second_device():
+    """Kernel attributes and grid sizes are per device: a handle on device 1
+    after device 0 was used factors correctly (skipped on one GPU)."""
+    import torch
+
+    from dalia_b200 import serinv_compat as sc
+
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one GPU")
+    D, L, Ab, T = bta_ref.random_bta(3, 130, 3, np.random.default_rng(2))
+    ref = [x.copy() for x in (D, L, Ab, T)]
+    bta_ref.pobtaf(*ref)
+    for dev in (0, 1):
+        with torch.cuda.device(dev):
+            d = [torch.from_numpy(x.copy()).cuda(dev) for x in (D, L, Ab, T)]
+            sc.pobtaf(*d)
+            for g, r in zip(d, ref):
+                assert rel(g.cpu().numpy(), r) < 1e-10

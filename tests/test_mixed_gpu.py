@@ -224,16 +224,20 @@ def test_i8slice_coregional_adjoint():
     assert abs(f - f64) < 1e-12 * max(1.0, abs(f64)) and rel(gr, g64) < 1e-6
 
 
+@pytest.mark.parametrize("tile", [0, 1])
 @pytest.mark.parametrize("case", GEMM_CASES)
-def test_gemm_i8slice_bit_exact_against_restatement(case):
+def test_gemm_i8slice_bit_exact_against_restatement(case, tile, monkeypatch):
     """The device's 8-bit-slice product equals the step-by-step CPU restatement
     of its arithmetic (oracle/ozaki_ref.py) bit for bit: digits and level sums
     are integers, the level combination is exact, and the one rounding
-    (hi + lo 2^-21) and the power-of-two scalings are the same."""
+    (hi + lo 2^-21) and the power-of-two scalings are the same.  Both output
+    tile widths the autotuner chooses from (64; 32 with two accumulator sets)."""
     import torch
 
     from dalia_b200 import _lib
     from oracle import ozaki_ref
+
+    monkeypatch.setenv("DALIA_B200_TUNE_FORCE", f"gemm_i8={tile}")
 
     lib = _lib.load()
     h = _lib.handle()
@@ -252,3 +256,48 @@ def test_gemm_i8slice_bit_exact_against_restatement(case):
         _lib.check(lib.bta_get_status(h.bind_stream(), ctypes.byref(st)), "status")
         got = dC.cpu().numpy()
         assert np.array_equal(got, exp), f"max diff {np.max(np.abs(got - exp))}"
+
+
+@pytest.mark.parametrize("n,b,a", [(4, 200, 6), (3, 300, 70), (5, 129, 0)])
+def test_factor_with_i8slice_schur_updates(n, b, a):
+    """bta_pobtaf_batched_ex with the previous-column Schur updates in 8-bit
+    slices: the factor, and the log-determinant from it, against the FP64
+    oracle (the updates are exact to ~1e-14 of sum |L||L|)."""
+    import torch
+
+    from dalia_b200 import _lib
+
+    lib = _lib.load()
+    h = _lib.handle()
+    D, L, Ab, T = bta_ref.random_bta(n, b, a, np.random.default_rng(n + b + a))
+    ref = [x.copy() for x in (D, L, Ab, T)]
+    bta_ref.pobtaf(*ref)
+    d = [torch.from_numpy(x.copy()).cuda() for x in (D, L, Ab, T)]
+    one = lambda v: (ctypes.c_int64 * 1)(v)  # noqa: E731
+    ptr = lambda t: (ctypes.c_void_p * 1)(t.data_ptr() if t.numel() else None)  # noqa: E731
+    info = ctypes.c_int64(-1)
+    rc = lib.bta_pobtaf_batched_ex(h.bind_stream(), 1, one(n), one(b), one(a), *[ptr(t) for t in d],
+                                   ctypes.byref(info), _lib.BTA_PREC_I8SLICE)
+    assert rc == 0 and info.value == 0
+    for g, r in zip(d, ref):
+        if r.size:
+            assert rel(g.cpu().numpy(), r) < 1e-11
+    ld = bta_ref.logdet(ref[0], ref[3] if a else None, "bta" if a else "bt")
+    ldg = bta_ref.logdet(d[0].cpu().numpy(), d[3].cpu().numpy() if a else None, "bta" if a else "bt")
+    assert abs(ldg - ld) <= 1e-12 * abs(ld)
+
+
+@pytest.mark.parametrize("name", ["gst_300x10", "gst_ragged"])
+def test_adjoint_with_i8slice_factor_updates(name):
+    """Both the factorisations' Schur updates and the selected inversion in
+    8-bit slices: f (hence the log-determinants) within 1e-10 of the FP64
+    path, the gradient within 1e-6."""
+    from dalia_b200.model import SpatioTemporalModel
+
+    g = load(name)
+    m = SpatioTemporalModel(problem(g), selinv_precision="i8slice", factor_precision="i8slice")
+    f64, g64 = m.objective_adjoint_batched([g["theta"]], precision="fp64")
+    fm, gm = m.objective_adjoint_batched([g["theta"]])
+    assert abs(fm[0] - f64[0]) <= 1e-10 * abs(f64[0])
+    assert rel(gm[0], g64[0]) < 1e-6
+    assert not m.last_check[0]["fallback"]

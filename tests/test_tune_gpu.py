@@ -1,0 +1,79 @@
+"""The online autotuner: every candidate launch configuration it chooses from
+gives the same results (the factorisation's queue lookahead and CTAs per SM,
+the persistent sweep's CTAs per SM and row segments), and a factorisation of
+a new shape records a decision after trying them."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from golden_util import rel
+from oracle import bta_ref
+
+pytestmark = pytest.mark.gpu
+
+
+def _factor(count, n, b, a, seed):
+    import torch
+
+    from dalia_b200 import _lib
+
+    lib = _lib.load()
+    h = _lib.handle()
+    mats = [bta_ref.random_bta(n, b, a, np.random.default_rng(seed + k)) for k in range(count)]
+    dev = [[torch.from_numpy(x.copy()).cuda() for x in m] for m in mats]
+    arr = lambda vals, t=ctypes.c_int64: (t * count)(*vals)  # noqa: E731
+    ptrs = [(ctypes.c_void_p * count)(*[d[j].data_ptr() for d in dev]) for j in range(4)]
+    info = ctypes.c_int64(-1)
+    rc = lib.bta_pobtaf_batched(h.bind_stream(), count, arr([n] * count), arr([b] * count), arr([a] * count), *ptrs,
+                                ctypes.byref(info))
+    assert rc == 0 and info.value == 0
+    return mats, dev
+
+
+@pytest.mark.parametrize("cand", range(6))
+def test_every_panel_candidate_factors_exactly(cand, monkeypatch):
+    monkeypatch.setenv("DALIA_B200_TUNE_FORCE", f"panel={cand}")
+    mats, dev = _factor(3, 6, 200, 5, 100 + cand)
+    for m, d in zip(mats, dev):
+        ref = [x.copy() for x in m]
+        bta_ref.pobtaf(*ref)
+        for g, r in zip(d, ref):
+            assert rel(g.cpu().numpy(), r) < 1e-10
+
+
+@pytest.mark.parametrize("cand", range(3))
+def test_every_sweep_candidate_solves_exactly(cand, monkeypatch):
+    import torch
+
+    from dalia_b200 import serinv_compat as sc
+
+    monkeypatch.setenv("DALIA_B200_TUNE_FORCE", f"sweep={cand}")
+    n, b, a = 5, 300, 4
+    D, L, Ab, T = bta_ref.random_bta(n, b, a, np.random.default_rng(9))
+    M = bta_ref.bta_to_dense(D, L, Ab, T)
+    d = [torch.from_numpy(x.copy()).cuda() for x in (D, L, Ab, T)]
+    sc.pobtaf(*d)
+    rhs = np.random.default_rng(10).standard_normal(n * b + a)
+    x = torch.from_numpy(rhs.copy()).cuda()
+    sc.pobtas(*d, x, "N")
+    sc.pobtas(*d, x, "C")
+    assert rel(x.cpu().numpy(), np.linalg.solve(M, rhs)) < 1e-10
+
+
+def test_tuner_decides_and_reports(monkeypatch):
+    """A batched factorisation with many block columns of one new shape: the
+    tuner tries the panel candidates on its block columns and records a
+    decision, still giving the exact factor."""
+    from dalia_b200 import _lib
+
+    monkeypatch.delenv("DALIA_B200_TUNE_FORCE", raising=False)
+    monkeypatch.delenv("DALIA_B200_TUNE", raising=False)
+    mats, dev = _factor(2, 20, 131, 3, 300)
+    for m, d in zip(mats, dev):
+        ref = [x.copy() for x in m]
+        bta_ref.pobtaf(*ref)
+        for g, r in zip(d, ref):
+            assert rel(g.cpu().numpy(), r) < 1e-10
+    lines = _lib.tune_report()
+    assert any(ln.startswith("panel|") and "best=" in ln for ln in lines), lines
