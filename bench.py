@@ -123,11 +123,16 @@ def config_of(name):
 
 
 # ----------------------------------------------------------------- CPU port
+_ORACLES = {}
+
+
 def cpu_sample(workload, nt_sample, reps=1):
     """Time one f(theta) of the CPU oracle on the workload truncated to
     nt_sample time steps; returns (seconds per full FD gradient, description,
     seconds of the sampled f).  A mixed-size batch is timed member by member
-    and weighted by its points per step (seconds per gradient, averaged)."""
+    and weighted by its points per step (seconds per gradient, averaged).
+    The oracle model of a (workload, nt) is built and warmed up once per
+    process."""
     from dalia_b200 import synth
     from oracle import coreg_ref, model_ref
 
@@ -139,12 +144,15 @@ def cpu_sample(workload, nt_sample, reps=1):
         cfg = dict(config_of(name))
         nt_full = cfg["nt"]
         cfg["nt"] = min(nt_sample, nt_full)
-        if coreg:
-            om = coreg_ref.CoregionalOracle(synth.make_coregional_problem(seed=0, **cfg))
-        else:
-            om = model_ref.OracleModel(synth.make_problem(seed=0, **cfg))
         th = np.asarray(cfg["theta"], dtype=np.float64)
-        om.evaluate_f(th)  # warm-up (BLAS thread pool, caches)
+        om = _ORACLES.get((name, cfg["nt"]))
+        if om is None:
+            if coreg:
+                om = coreg_ref.CoregionalOracle(synth.make_coregional_problem(seed=0, **cfg))
+            else:
+                om = model_ref.OracleModel(synth.make_problem(seed=0, **cfg))
+            om.evaluate_f(th)  # warm-up (BLAS thread pool, caches)
+            _ORACLES[(name, cfg["nt"])] = om
         ts = []
         for _ in range(reps):
             t0 = time.perf_counter()
