@@ -45,7 +45,7 @@ SIGNATURES = {
     "bta_pobtaf_batched": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
                                   _c_void_p, _pi64]),
     "bta_pobtaf_batched_ex": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
-                                     _c_void_p, _c_void_p, _c_void_p, _pi64, _int]),
+                                     _c_void_p, _c_void_p, _pi64, _int]),
     "bta_pobtas_batched": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
                                   _c_void_p, _c_void_p, _int]),
     "bta_pobtasi_batched": (_int, [_c_void_p, _int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,

@@ -278,7 +278,8 @@ class SpatioTemporalModel:
         self.Qp = BTAMatrix(n, b, 0, dev)
         self._dev = dev
         first, second, row_of_p = _pairs_per_row(A)
-        c1, c2 = A.indices[first], A.indices[second]
+        # 64-bit positions: a BTA array of 250 blocks of 4000 x 4000 has 4e9 entries
+        c1, c2 = A.indices[first].astype(np.int64), A.indices[second].astype(np.int64)
         fac = A.data[first] * A.data[second]
         obs = row_of_p[first]
         nbt = n * b

@@ -69,10 +69,10 @@ def test_univariate_assembly_matches_reference(name):
 
 @pytest.mark.parametrize("name", ["gst_coreg3_small", "gst_coreg2_ragged"])
 def test_coregional_assembly_matches_reference(name):
-    """The reference orders the latent vector variate by variate; the device
-    interleaves the variates per time step (a fixed permutation of rows and
-    columns, ``latent_permutation``)."""
-    from dalia_b200.coregional import CoregionalModel, latent_permutation
+    """The reference's coregional matrices are stored in its permuted order
+    (variates interleaved per time step, fixed effects last,
+    ``coregional_model.py:750-853``), which is the device's BTA order."""
+    from dalia_b200.coregional import CoregionalModel
 
     g = load(name)
     m = CoregionalModel(coreg_problem(g))
@@ -81,7 +81,6 @@ def test_coregional_assembly_matches_reference(name):
     m._gauss_conditional(th, sl)
     m.assemble_prior_bt(th, sl)
     N = m.N
-    perm = latent_permutation(m.nt, m.ns, m.nv, m.nb // m.nv)
-    Qc = sps.coo_matrix((g["qc_data"], (g["qc_row"], g["qc_col"])), shape=(N, N)).tocsr()[perm][:, perm]
-    Qp = sps.coo_matrix((g["qp_data"], (g["qp_row"], g["qp_col"])), shape=(N, N)).tocsr()[perm][:, perm]
+    Qc = sps.coo_matrix((g["qc_data"], (g["qc_row"], g["qc_col"])), shape=(N, N))
+    Qp = sps.coo_matrix((g["qp_data"], (g["qp_row"], g["qp_col"])), shape=(N, N))
     _check(m, g, Qc, Qp)

@@ -62,7 +62,10 @@ def test_fp64_path_matches_oracle_at_full_size(name):
     D, L, Ab, T = sel
     mv_ref = np.concatenate([np.concatenate([np.diagonal(D[i]) for i in range(m.nt)]), np.diagonal(T)])
     assert rel(mv, mv_ref) < TOL
-    assert float(np.max(np.abs(mv - mv_ref) / np.abs(mv_ref))) < TOL
+    # entry by entry the smallest variances (1e-6 of the largest) carry the
+    # rounding of the recurrence relative to their own size: measured up to
+    # 1e-9 between two FP64 evaluations in different operation orders
+    assert float(np.max(np.abs(mv - mv_ref) / np.abs(mv_ref))) < 1e-8
     # the selected inverse on the BTA pattern (DALIA reads the lower
     # triangles of the diagonal blocks, the sub-diagonal and arrow blocks)
     Q = m.slots[0].Qc
