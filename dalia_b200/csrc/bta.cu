@@ -601,10 +601,11 @@ int bta_pobtasi_batched_ex(bta_handle_t h, int count, const int64_t* n, const in
 
 // Blocks whose inverses one instance computes at a time when the caller does
 // not supply them: the inverses are made chunk by chunk as the backward
-// recurrence reaches them, so the workspace holds C blocks instead of n.
+// recurrence reaches them, so the workspace holds C blocks (at most 2 GiB)
+// instead of n.
 inline int64_t inverse_chunk(int64_t n, int64_t b) {
   const int64_t per = b * b * 8;
-  return std::max<int64_t>(1, std::min<int64_t>(n, (int64_t(512) << 20) / per));
+  return std::max<int64_t>(1, std::min<int64_t>(n, (int64_t(2048) << 20) / per));
 }
 
 int bta_pobtasi_batched_v(bta_handle_t h, int count, const int64_t* n, const int64_t* b, const int64_t* a,

@@ -122,7 +122,7 @@ int bta_pobtaf_batched_ex(bta_handle_t h, int count, const int64_t* n, const int
  * selected inversion skips its own block inversion
  * (bta_pobtasi_batched_v; V == NULL, or V[k] == NULL for one instance,
  * computes them as bta_pobtasi_batched_ex does: chunk by chunk as the
- * recurrence reaches them, in at most 512 MiB of workspace per instance).
+ * recurrence reaches them, in at most 2 GiB of workspace per instance).
  * No counterpart in the reference: Serinv's pobtas solves with the factor
  * blocks directly.
  */

