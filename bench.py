@@ -6,7 +6,8 @@ nt = 100, nb = 6, 600 observations per step; BTA blocks 1500 x 1500).
                     [--workload NAME] [--batch K] [--precision fp64|i8slice|tf32x3]
 
 One step = full gradient evaluations (f(theta) and grad f) at ``--batch``
-theta points (the candidates of a line search, default 3), the unit counted
+theta points (candidates of a line search or points of a stencil, default
+6), the unit counted
 being one gradient evaluation.  ``ours`` uses the adjoint path (one
 factorisation and selected inversion of Q_c and of Q_prior per point, all 2K
 matrices factored and inverted together); the single-point adjoint and the
@@ -58,9 +59,9 @@ def parse(argv=None):
                    help="reference arm: also time one f(theta) on the untruncated workload (0: skip)")
     p.add_argument("--fd-steps", type=int, default=3, help="timed repeats of each FD path (after one warm-up)")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU-oracle baseline sample")
-    p.add_argument("--batch", type=int, default=3,
-                   help="theta points per step (a line-search batch), factorised together; "
-                        "reduced to what device memory holds")
+    p.add_argument("--batch", type=int, default=6,
+                   help="theta points per step (e.g. line-search candidates or stencil points), factorised "
+                        "together; reduced to what device memory holds")
     p.add_argument("--precision", default="i8slice", choices=["fp64", "tf32x3", "i8slice"],
                    help="arithmetic of the selected inversions behind the adjoint gradient")
     p.add_argument("--factor-precision", default="fp64", choices=["fp64", "i8slice"],

@@ -112,49 +112,34 @@ __global__ void tip_final_kernel(int nparts, int a, const double* part, double p
 // out[blk][v][w][K] = sum over the union pattern of sub-block (v, w) of block
 // blk of S[v ns + s][w ns + c] * K[s][c] (blk < n: diagonal block D_t; else
 // sub-diagonal block L_{blk-n}).  One CTA per (blk, v, w).
-// The four values of one union-pattern entry (one 32-byte load when aligned).
-__device__ __forceinline__ double4 load4(const double* p, bool aligned) {
-  if (aligned) return *reinterpret_cast<const double4*>(p);
-  return make_double4(p[0], p[1], p[2], p[3]);
-}
-
 __global__ void __launch_bounds__(256) block_inner_kernel(int n, int ns, int nv, const int* rowptr,
                                                           const int* colidx, const double* vals4, const double* D,
                                                           const double* L, double* out) {
-  __shared__ double red[4][8];
+  __shared__ double red[4][256];
   const int blk = blockIdx.x / (nv * nv), vw = blockIdx.x % (nv * nv), v = vw / nv, w = vw % nv;
   const int b = nv * ns;
   const bool lower = blk >= n;
   const int t = lower ? blk - n : blk;
   const double* M = (lower ? L + (size_t)t * b * b : D + (size_t)t * b * b) + (size_t)v * ns * b + w * ns;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const bool v4 = (reinterpret_cast<uintptr_t>(vals4) & 31) == 0;
-  // a warp per row: its lanes read the row's pattern entries, which lie in a
-  // few neighbouring sectors (mesh neighbours), instead of 32 rows at once
   double s[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int row = warp; row < ns; row += 8) {
-    const double* Mr = M + (size_t)row * b;
-    for (int e = rowptr[row] + lane; e < rowptr[row + 1]; e += 32) {
-      const double m = Mr[colidx[e]];
-      const double4 vv = load4(vals4 + (size_t)e * 4, v4);
-      s[0] += m * vv.x;
-      s[1] += m * vv.y;
-      s[2] += m * vv.z;
-      s[3] += m * vv.w;
+  for (int row = threadIdx.x; row < ns; row += blockDim.x) {
+    for (int e = rowptr[row]; e < rowptr[row + 1]; ++e) {
+      const double m = M[(size_t)row * b + colidx[e]];
+      const double* vv = vals4 + (size_t)e * 4;
+      s[0] += m * vv[0];
+      s[1] += m * vv[1];
+      s[2] += m * vv[2];
+      s[3] += m * vv[3];
     }
   }
-#pragma unroll
-  for (int k = 0; k < 4; ++k)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
-  if (lane == 0)
-    for (int k = 0; k < 4; ++k) red[k][warp] = s[k];
+  for (int k = 0; k < 4; ++k) red[k][threadIdx.x] = s[k];
   __syncthreads();
-  if (threadIdx.x < 4) {
-    double a = 0.0;
-    for (int q = 0; q < 8; ++q) a += red[threadIdx.x][q];
-    out[(size_t)blockIdx.x * 4 + threadIdx.x] = a;
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int k = 0; k < 4; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + o];
+    __syncthreads();
   }
+  if (threadIdx.x < 4) out[(size_t)blockIdx.x * 4 + threadIdx.x] = red[threadIdx.x][0];
 }
 
 // out[blk][v][w][K] = x_{r,v}^T K x_{c,w} over the union pattern, where x_{t,v}
@@ -163,39 +148,33 @@ __global__ void __launch_bounds__(256) block_inner_kernel(int n, int ns, int nv,
 __global__ void __launch_bounds__(256) block_quad_kernel(int n, int ns, int nv, const int* rowptr,
                                                          const int* colidx, const double* vals4, const double* x,
                                                          double* out) {
-  __shared__ double red[4][8];
+  __shared__ double red[4][256];
   const int blk = blockIdx.x / (nv * nv), vw = blockIdx.x % (nv * nv), v = vw / nv, w = vw % nv;
   const int b = nv * ns;
   const bool lower = blk >= n;
   const int t = lower ? blk - n : blk;
   const double* xr = x + (size_t)(lower ? t + 1 : t) * b + v * ns;
   const double* xc = x + (size_t)t * b + w * ns;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const bool v4 = (reinterpret_cast<uintptr_t>(vals4) & 31) == 0;
   double s[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int row = warp; row < ns; row += 8) {
+  for (int row = threadIdx.x; row < ns; row += blockDim.x) {
     const double xv = xr[row];
-    for (int e = rowptr[row] + lane; e < rowptr[row + 1]; e += 32) {
+    for (int e = rowptr[row]; e < rowptr[row + 1]; ++e) {
       const double m = xv * xc[colidx[e]];
-      const double4 vv = load4(vals4 + (size_t)e * 4, v4);
-      s[0] += m * vv.x;
-      s[1] += m * vv.y;
-      s[2] += m * vv.z;
-      s[3] += m * vv.w;
+      const double* vv = vals4 + (size_t)e * 4;
+      s[0] += m * vv[0];
+      s[1] += m * vv[1];
+      s[2] += m * vv[2];
+      s[3] += m * vv[3];
     }
   }
-#pragma unroll
-  for (int k = 0; k < 4; ++k)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
-  if (lane == 0)
-    for (int k = 0; k < 4; ++k) red[k][warp] = s[k];
+  for (int k = 0; k < 4; ++k) red[k][threadIdx.x] = s[k];
   __syncthreads();
-  if (threadIdx.x < 4) {
-    double a = 0.0;
-    for (int q = 0; q < 8; ++q) a += red[threadIdx.x][q];
-    out[(size_t)blockIdx.x * 4 + threadIdx.x] = a;
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int k = 0; k < 4; ++k) red[k][threadIdx.x] += red[k][threadIdx.x + o];
+    __syncthreads();
   }
+  if (threadIdx.x < 4) out[(size_t)blockIdx.x * 4 + threadIdx.x] = red[threadIdx.x][0];
 }
 
 // out[blockIdx] partial of sum_e w[e] * base[idx[e]]
