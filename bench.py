@@ -64,8 +64,9 @@ def parse(argv=None):
                         "together; reduced to what device memory holds")
     p.add_argument("--precision", default="i8slice", choices=["fp64", "tf32x3", "i8slice"],
                    help="arithmetic of the selected inversions behind the adjoint gradient")
-    p.add_argument("--factor-precision", default="fp64", choices=["fp64", "i8slice"],
-                   help="arithmetic of the factorisations' previous-column Schur updates in the adjoint path")
+    p.add_argument("--factor-precision", default="i8slice", choices=["fp64", "i8slice"],
+                   help="arithmetic of the factorisations' previous-column Schur updates in the adjoint path "
+                        "(with --precision fp64 the whole path is FP64)")
     return p.parse_args(argv)
 
 
@@ -422,15 +423,18 @@ def run_ours(args):
     run_step(nwarm + 2 * args.steps)
     lib.bta_prof_enable(0)
     lib.bta_prof_read(pre_ms, pre_cnt)
-    # the 8-bit-slice GEMM's digit pre-pass counts towards the GEMM's time
-    dom = max((0, 1), key=lambda c: pre_ms[0] if c == 0 else pre_ms[1] + pre_ms[5])
+    # kernel groups: 0 the panel kernel, 1 the selected inversion's GEMM, 2 the
+    # factorisation's Schur-update GEMM (reduced-precision factor updates);
+    # an 8-bit-slice GEMM's digit pre-pass counts towards its GEMM's time
+    groups = {0: (0,), 1: (1, 5), 2: (6,)}
+    dom = max(groups, key=lambda g: sum(pre_ms[c] for c in groups[g]))
     barrier()
 
     # ---- device-timed steps: K-point adjoint gradient batches (events around
     # the dominant category's launches)
     clock = ClockSampler(local)
     clock.start()
-    lib.bta_prof_mask(1 if dom == 0 else (1 << 1) | (1 << 5))
+    lib.bta_prof_mask(sum(1 << c for c in groups[dom]))
     lib.bta_prof_enable(1)
     launches0 = lib.bta_launch_count()
     work0 = work_sum()
@@ -526,31 +530,34 @@ def run_ours(args):
     fd_seq = fd_rate(False) if args.fd_steps > 0 else None
     fd_bat = fd_rate(True) if args.fd_steps > 0 else None
 
-    # ---- roofline of the dominant kernel category
+    # ---- roofline of the dominant kernel group
     names = {0: "panel (tile-DAG BTA panel Cholesky)",
              1: {"fp64": "gemm (grouped FP64 DMMA GEMM)",
                  "tf32x3": "gemm (split-TF32 tcgen05 GEMM)",
-                 "i8slice": "gemm (8-bit-slice tcgen05 GEMM incl. digit pre-pass)"}[args.precision]}
+                 "i8slice": "gemm (8-bit-slice tcgen05 GEMM incl. digit pre-pass)"}[args.precision],
+             2: "gemm (8-bit-slice tcgen05 GEMM of the factorisation's Schur updates incl. digit pre-pass)"}
     # algorithmic flops issued in the timed region (every Newton factorisation
     # of a non-Gaussian likelihood included)
-    tot_flops = {0: work["factor"], 1: work["selinv_gemm"]}
-    cat_ms = {0: ms_cat[0], 1: ms_cat[1] + ms_cat[5]}
+    tot_flops = {0: work["factor"] - work["factor_schur"], 1: work["selinv_gemm"], 2: work["factor_schur"]}
+    cat_ms = {g: sum(ms_cat[c] for c in cs) for g, cs in groups.items()}
     achieved = tot_flops[dom] / (cat_ms[dom] * 1e-3) / 1e12
     # launch shape of the first member: block, arrow, matrices per launch
     shape = (model.b, model.nb, 2 * Ks[0])
     traffic, traffic_src = roofline_traffic(args.workload, names[dom].split()[0], shape)
     dom_peak, peak_src = peak, "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor pipe)"
-    if dom == 1 and args.precision == "i8slice":
+    try:
+        bf16 = float(json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))["bf16_tflops"])
+        bf16_src = "measured"
+    except Exception:
+        bf16, bf16_src = 1590.0, "fallback"
+    if (dom == 1 and args.precision == "i8slice") or dom == 2:
         # FP64-equivalent ceiling of 28 int8 digit products per product: the
-        # dense int8 rate taken as twice the measured bf16 burst
-        try:
-            bf16 = float(json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))["bf16_tflops"])
-            src = "measured"
-        except Exception:
-            bf16, src = 1590.0, "fallback"
+        # dense int8 rate taken as twice the bf16 burst
         dom_peak = 2 * bf16 / 28
-        peak_src = (f"2 x {src} bf16 burst ({bf16:.0f} TF/s) / 28 digit products "
+        peak_src = (f"2 x {bf16_src} bf16 burst ({bf16:.0f} TF/s) / 28 digit products "
                     f"(int8 ceiling, FP64-equivalent)")
+    # the panel kernel's own rate in the profiled step, whichever group dominates
+    panel_rate = tot_flops[0] / args.steps / max(pre_ms[0] * 1e-3, 1e-12) / 1e12
     roofline = {
         "bound": "tensor",
         "kernel": names[dom],
@@ -559,13 +566,14 @@ def run_ours(args):
         "unit": "TFLOP/s",
         "frac": achieved / dom_peak,
         "peak_source": peak_src,
-        "avg_launch_ms": cat_ms[dom] / max(cnt_cat[dom], 1),
-        "launches": int(cnt_cat[dom]),
+        "avg_launch_ms": cat_ms[dom] / max(cnt_cat[groups[dom][0]], 1),
+        "launches": int(cnt_cat[groups[dom][0]]),
         "traffic": traffic,
         "traffic_source": traffic_src,
     }
     # per-category split of the profiled step (events around every launch)
-    kernel_ms = {k: pre_ms[i] for i, k in enumerate(["panel", "gemm", "sweep", "trtri", "other", "slice"])}
+    kernel_ms = {k: pre_ms[i] for i, k in enumerate(["panel", "gemm", "sweep", "trtri", "other", "slice",
+                                                    "factor_gemm"])}
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -623,7 +631,10 @@ def run_ours(args):
             "speedup_vs_fd_fp64": (value / fd_seq) if fd_seq else None,
             "speedup_vs_fd_fp64_batched": (value / fd_bat) if fd_bat else None,
             # per-step work of the timed region over the profiled step's kernel times
-            "bta_factor_tflops": tot_flops[0] / args.steps / max(pre_ms[0] * 1e-3, 1e-12) / 1e12,
+            "bta_factor_tflops": work["factor"] / args.steps / max((pre_ms[0] + pre_ms[6]) * 1e-3, 1e-12) / 1e12,
+            "panel_roofline": {"achieved": panel_rate, "peak": peak, "unit": "TFLOP/s", "frac": panel_rate / peak,
+                               "source": "profiled step; algorithmic flops of the panel kernel's share of the "
+                                         "factorisation over its time, vs the in-run cuBLAS DGEMM"},
             "bta_selinv_gemm_tflops": tot_flops[1] / args.steps / max((pre_ms[1] + pre_ms[5]) * 1e-3, 1e-12) / 1e12,
             "kernel_ms_source": "one profiled step before the timed region (events around every launch); "
                                 "in the timed region only the roofline kernel's launches carry events",

@@ -418,7 +418,10 @@ int bta_pobtaf_batched_ex(bta_handle_t h, int count, const int64_t* n, const int
           sch.push_back(q);
         }
       }
-      if (!sch.empty() && (rc = run_gemm(h, sch, precision))) return rc;
+      if (!sch.empty()) {
+        ProfRetarget rt(PROF_FACTOR_GEMM);
+        if ((rc = run_gemm(h, sch, precision))) return rc;
+      }
     }
   }
   std::vector<PanelSpec> tips;

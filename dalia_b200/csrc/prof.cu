@@ -69,6 +69,20 @@ int device_sm_count() {
   return it->second;
 }
 
+namespace {
+thread_local int t_retarget = -1;
+}  // namespace
+
+int prof_retarget(int cat) {
+  const int prev = t_retarget;
+  t_retarget = cat;
+  return prev;
+}
+
+int prof_category(int cat) {
+  return (t_retarget >= 0 && (cat == PROF_GEMM || cat == PROF_SLICE)) ? t_retarget : cat;
+}
+
 void prof_begin(int cat, cudaStream_t s, cudaEvent_t* ev) {
   g_launches.fetch_add(1, std::memory_order_relaxed);
   *ev = nullptr;

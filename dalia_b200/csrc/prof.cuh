@@ -7,7 +7,9 @@
 
 namespace bta {
 
-// PROF_SLICE: the digit pre-pass of the 8-bit-slice GEMM
+// PROF_SLICE: the digit pre-pass of the 8-bit-slice GEMM; PROF_FACTOR_GEMM:
+// the GEMMs (and their pre-pass) that apply the factorisation's
+// previous-column Schur updates when those run outside the panel kernel.
 enum ProfCat : int {
   PROF_PANEL = 0,
   PROF_GEMM = 1,
@@ -15,8 +17,19 @@ enum ProfCat : int {
   PROF_TRTRI = 3,
   PROF_OTHER = 4,
   PROF_SLICE = 5,
+  PROF_FACTOR_GEMM = 6,
   PROF_NCAT = 8
 };
+
+// While a ProfRetarget lives on this thread, GEMM and pre-pass launches
+// count under the given category.
+int prof_retarget(int cat);  // returns the previous target (-1: none)
+struct ProfRetarget {
+  int prev;
+  explicit ProfRetarget(int cat) : prev(prof_retarget(cat)) {}
+  ~ProfRetarget() { prof_retarget(prev); }
+};
+int prof_category(int cat);
 
 void prof_begin(int cat, cudaStream_t s, cudaEvent_t* ev);
 void prof_end(int cat, cudaStream_t s, cudaEvent_t ev);
@@ -35,7 +48,7 @@ struct ProfScope {
   int cat;
   cudaStream_t s;
   cudaEvent_t ev = nullptr;
-  ProfScope(int c, cudaStream_t st) : cat(c), s(st) { prof_begin(cat, s, &ev); }
+  ProfScope(int c, cudaStream_t st) : cat(prof_category(c)), s(st) { prof_begin(cat, s, &ev); }
   ~ProfScope() { prof_end(cat, s, ev); }
 };
 

@@ -328,7 +328,9 @@ class SpatioTemporalModel:
         self.slots = [self._new_slot(self.Qc, self.Qp)]
         # algorithmic flops of the factorisations / selected-inversion GEMMs
         # issued so far, and Newton steps taken (non-Gaussian likelihoods)
-        self.work = {"factor": 0.0, "selinv_gemm": 0.0, "newton_steps": 0}
+        # (factor_schur: the part of "factor" applied by GEMMs outside the panel
+        # kernel when the Schur updates run in reduced precision)
+        self.work = {"factor": 0.0, "factor_schur": 0.0, "selinv_gemm": 0.0, "newton_steps": 0}
 
     def _new_slot(self, Qc=None, Qp=None):
         return _Slot(self.nt, self.b, self.nb, self.N, self.nobs, self._dev, Qc, Qp, self.nv)
@@ -461,6 +463,8 @@ class SpatioTemporalModel:
         """All matrices factored together, block column by block column;
         precision: arithmetic of the previous-column Schur updates."""
         self.work["factor"] += sum(factor_flops(m.n, m.b, m.a) for m in mats)
+        if precision != "fp64":
+            self.work["factor_schur"] += sum((m.n - 1) * (m.b ** 3 + 2 * m.a * m.b ** 2) for m in mats)
         k, n, b, a, D, L, Ab, T = self._batched_args(mats)
         self._check(self.lib.bta_pobtaf_batched_ex(self.h.bind_stream(), k, n, b, a, D, L, Ab, T, None,
                                                    _PRECISIONS[precision]), "pobtaf_batched")

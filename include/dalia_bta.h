@@ -237,7 +237,9 @@ size_t bta_noalloc_scratch_bytes(void);
  * kernels): total kernel launches of this library in the process, and
  * optional per-category device time from CUDA events recorded around every
  * launch on its stream.  Categories: 0 panel factorisation, 1 GEMM, 2 solve
- * sweeps, 3 block inverses, 4 other.  bta_prof_enable(1) creates the
+ * sweeps, 3 block inverses, 4 other, 5 digit pre-pass of the 8-bit-slice
+ * GEMM, 6 the factorisation's Schur-update GEMMs (with their pre-pass) when
+ * they run outside the panel kernel (bta_pobtaf_batched_ex).  bta_prof_enable(1) creates the
  * events beforehand (for about 8000 launches), so a timed region pays no
  * event creation; bta_prof_mask limits the events to the categories whose
  * bits are set (default: all), since events around every launch slow a step

@@ -35,4 +35,4 @@ def test_traffic_of_another_shape_is_scaled_by_algorithmic_bytes():
 def test_default_arguments():
     a = bench.parse([])
     assert (a.workload, a.batch, a.precision, a.factor_precision, a.fd_steps) == \
-        ("gst_1500x100", 6, "i8slice", "fp64", 3)
+        ("gst_1500x100", 6, "i8slice", "i8slice", 3)
