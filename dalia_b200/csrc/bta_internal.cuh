@@ -31,7 +31,6 @@ struct SweepBatch {
 };
 
 int diag_tile_inverses(const double* D, int n, int b, double* out, cudaStream_t s);
-int sweep_launch(const SweepArgs& A, cudaStream_t s);
 int sweep_launch_batched(SweepBatch& B, cudaStream_t s);
 // part: n * a doubles of scratch.
 int arrow_forward(const double* Ab, const double* T, double* x, int n, int b, int a, double* part, cudaStream_t s);

@@ -413,15 +413,6 @@ int sweep_launch_batched(SweepBatch& B, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-int sweep_launch(const SweepArgs& A, cudaStream_t s) {
-  SweepBatch B;
-  std::memset(&B, 0, sizeof(B));
-  B.count = 1;
-  B.counter = A.counter;
-  B.inst[0] = A;
-  return sweep_launch_batched(B, s);
-}
-
 int arrow_forward(const double* Ab, const double* Tt, double* x, int n, int b, int a, double* part,
                   cudaStream_t s) {
   if (a <= 0) return cudaSuccess;
