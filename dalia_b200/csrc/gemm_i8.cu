@@ -409,6 +409,7 @@ struct QProb {
   const int* eA;  // M row exponents
   const int* fB;  // N column exponents
   double beta;
+  double sgn;     // +1, or -1 when a one-segment product's alpha = -1 is applied here
   int ldc, M, N, nseg, cflags, tmn, tnn;
   QSeg seg[3];
 };
@@ -661,14 +662,14 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
             for (int j = 0; j < 16; ++j) {
               const double sc = __shfl_sync(0xffffffffu, scol, 16 * h + j);
               const double v = fma(exact_double(lo[j]), 0x1p-21, exact_double(hi[j]));
-              stage[lane * QSTAGE_LD + 32 * c + 16 * h + j] = (v * srow) * sc;
+              stage[lane * QSTAGE_LD + 32 * c + 16 * h + j] = ((v * srow) * sc) * P.sgn;
             }
           } else {
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
               const int fc = __shfl_sync(0xffffffffu, fcol, 16 * h + j);
               const double v = fma(exact_double(lo[j]), 0x1p-21, exact_double(hi[j]));
-              stage[lane * QSTAGE_LD + 32 * c + 16 * h + j] = ldexp(v, er + fc - 35);
+              stage[lane * QSTAGE_LD + 32 * c + 16 * h + j] = ldexp(v, er + fc - 35) * P.sgn;
             }
           }
         }
@@ -770,6 +771,12 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
     q.M = p.M;
     q.N = p.N;
     q.beta = p.beta;
+    // the digits of -x are those of x negated (|x| is cut, the sign kept
+    // apart), so a one-segment product with alpha = -1 cuts A unscaled and
+    // negates in the epilogue -- bit for bit the same result -- and A can
+    // then share its digit images with an equal B side (D -= L L^T cuts L once)
+    const bool neg1 = p.nseg == 1 && p.seg[0].alpha == -1.0;
+    q.sgn = neg1 ? -1.0 : 1.0;
     q.cflags = p.cflags;
     q.nseg = p.nseg;
     q.tmn = (p.M + QBM - 1) / QBM;
@@ -785,7 +792,7 @@ int gemm_launch_i8(const std::vector<GemmProb>& probs, cudaStream_t stream, int*
     for (int s = 0; s < p.nseg; ++s) {
       const GemmSeg& g = p.seg[s];
       const int KT = (g.K + QBK - 1) / QBK;
-      ga.s[s] = SliceSeg{g.A, nullptr, g.alpha, g.lda, g.K, (g.flags & GF_A_T) ? 0 : 1, KT};
+      ga.s[s] = SliceSeg{g.A, nullptr, neg1 ? 1.0 : g.alpha, g.lda, g.K, (g.flags & GF_A_T) ? 0 : 1, KT};
       gb.s[s] = SliceSeg{g.B, nullptr, 1.0, g.ldb, g.K, (g.flags & GF_B_KN) ? 0 : 1, KT};
     }
     // a side equal to one already planned in this launch (same operands,

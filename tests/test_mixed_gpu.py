@@ -301,3 +301,29 @@ def test_adjoint_with_i8slice_factor_updates(name):
     assert abs(fm[0] - f64[0]) <= 1e-10 * abs(f64[0])
     assert rel(gm[0], g64[0]) < 1e-6
     assert not m.last_check[0]["fallback"]
+
+
+@pytest.mark.parametrize("M,K", [(300, 257), (1500, 1500)])
+def test_gemm_i8slice_syrk_bit_exact(M, K):
+    """C -= A A^T (lower, beta = 1) with the same array as both operands, the
+    factorisation's Schur update: the negation moves to the epilogue and A's
+    digits are cut once for both sides; the result equals the restatement bit
+    for bit."""
+    import torch
+
+    from dalia_b200 import _lib
+    from oracle import ozaki_ref
+
+    lib = _lib.load()
+    h = _lib.handle()
+    rng = np.random.default_rng(M + K)
+    A = rng.standard_normal((M, K)) * np.exp(-3.0 * rng.random((M, K)))
+    C = rng.standard_normal((M, M))
+    exp = ozaki_ref.gemm([(A, A, -1.0)], M, M, 1.0, C, True, False)
+    dA, dC = (torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (A, C))
+    _lib.check(lib.bta_gemm(h.bind_stream(), _lib.BTA_PREC_I8SLICE, M, M, K, -1.0, _lib.ptr(dA), K, 0,
+                            _lib.ptr(dA), K, 0, 1.0, _lib.ptr(dC), M, 1, 0), "gemm")
+    st = ctypes.c_int64(0)
+    _lib.check(lib.bta_get_status(h.bind_stream(), ctypes.byref(st)), "status")
+    got = dC.cpu().numpy()
+    assert np.array_equal(got, exp), f"max diff {np.max(np.abs(got - exp))}"
