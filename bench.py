@@ -64,9 +64,10 @@ def parse(argv=None):
                         "together; reduced to what device memory holds")
     p.add_argument("--precision", default="i8slice", choices=["fp64", "tf32x3", "i8slice"],
                    help="arithmetic of the selected inversions behind the adjoint gradient")
-    p.add_argument("--factor-precision", default="i8slice", choices=["fp64", "i8slice"],
+    p.add_argument("--factor-precision", default="auto", choices=["fp64", "i8slice", "auto"],
                    help="arithmetic of the factorisations' previous-column Schur updates in the adjoint path "
-                        "(with --precision fp64 the whole path is FP64)")
+                        "(auto: 8-bit slices for blocks of 1500 and wider; with --precision fp64 the whole "
+                        "path is FP64)")
     return p.parse_args(argv)
 
 
@@ -368,6 +369,10 @@ def run_ours(args):
         thetas.append(replica_theta(config_of(name)["theta"], rank))
         Ks.append(k if k is not None else max(1, args.batch))
     mixed = len(models) > 1
+    # the arithmetic the factorisations' Schur updates run in ("auto" resolved)
+    from dalia_b200.model import _factor_arith
+    factor_arith = _factor_arith(args.factor_precision, models, args.precision)
+    factor_desc = factor_arith if args.factor_precision != "auto" else f"{factor_arith} (auto by block size)"
     if not mixed:
         # Q_c, Q_prior and Q_c's block inverses of every point stay resident
         m = models[0]
@@ -502,7 +507,7 @@ def run_ours(args):
             "solution_rel_err_vs_fp64": float(np.linalg.norm(xr - x64) / np.linalg.norm(x64)),
             "selinv_diag_rel_err_vs_fp64": float(np.max(np.abs(sr - s64) / np.abs(s64))),
             "note": ("the factorisations' Schur updates and the selected inversion's block products differ; "
-                     "POTRF, log-determinant sums and sweeps are FP64 in both") if args.factor_precision != "fp64"
+                     "POTRF, log-determinant sums and sweeps are FP64 in both") if factor_arith != "fp64"
             else "factorisations, log-determinants and solves are FP64 in both; the selected inversion's "
                  "block products differ",
         })
@@ -598,7 +603,7 @@ def run_ours(args):
             "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else (
                 f"f64 + {args.precision} selected-inversion products"
-                + (f" + {args.factor_precision} factor Schur updates" if args.factor_precision != "fp64" else "")),
+                + (f" + {factor_arith} factor Schur updates" if factor_arith != "fp64" else "")),
             "data": "synthetic",
             "config": {
                 "workload": args.workload,
@@ -607,7 +612,7 @@ def run_ours(args):
                 "obs_per_step": cfg0["no"],
                 "theta": list(cfg0["theta"]),
                 "path": f"adjoint gradient, selected inversion in {args.precision}, factorisations' Schur updates "
-                        f"in {args.factor_precision if args.precision != 'fp64' else 'fp64'} (POTRF, log-dets, "
+                        f"in {factor_desc} (POTRF, log-dets, "
                         f"solves FP64); {units} theta points per step, theta moved between steps; Q_c and Q_prior of all "
                         f"points factorised and selected-inverted together"
                         + ("; members of different block sizes share every launch" if mixed else ""),

@@ -115,6 +115,22 @@ def selinv_gemm_flops(n, b, a):
 
 _PRECISIONS = {"fp64": _lib.BTA_PREC_FP64, "tf32x3": _lib.BTA_PREC_TF32X3, "i8slice": _lib.BTA_PREC_I8SLICE}
 
+# Smallest block size at which the factorisation's Schur updates as 8-bit-slice
+# GEMMs beat the FP64 updates inside the panel kernel (measured on B200: faster
+# at b = 1500 and 1800, slower for a batch of b = 1200 and 600 blocks).
+AUTO_I8_FACTOR_MIN_BLOCK = 1500
+
+
+def _factor_arith(requested, models, precision):
+    """Arithmetic of the Schur updates of a forward evaluation: FP64 whenever
+    the selected inversion is FP64 (a fully FP64 evaluation, e.g. the
+    fallback), else the model's choice, "auto" resolved by block size."""
+    if precision == "fp64" or requested == "fp64":
+        return "fp64"
+    if requested == "auto":
+        return "i8slice" if min(m.b for m in models) >= AUTO_I8_FACTOR_MIN_BLOCK else "fp64"
+    return requested
+
 
 class BTAMatrix:
     """One BTA matrix in a single device allocation with D, L, Ab, T views."""
@@ -185,10 +201,13 @@ class SpatioTemporalModel:
         tcgen05 tensor cores) or "i8slice" (8-bit digit products accumulated
         exactly in INT32 on the tensor cores, ~1e-10 relative).
         factor_precision: arithmetic of the factorisations' previous-column
-        Schur updates in a reduced-precision adjoint evaluation ("fp64" or
-        "i8slice"; the diagonal-block POTRF, the triangular solves, the
-        log-determinants and the sweeps stay FP64, and the plain f / FD paths
-        always factor in FP64).  Every adjoint evaluation checks its selected
+        Schur updates in a reduced-precision adjoint evaluation ("fp64",
+        "i8slice", or "auto": 8-bit slices when every block of the batch is at
+        least AUTO_I8_FACTOR_MIN_BLOCK wide, where they measured faster than the
+        FP64 updates fused into the panel kernel; the diagonal-block POTRF,
+        the triangular solves, the log-determinants and the sweeps stay FP64,
+        and the plain f / FD paths always factor in FP64).  Every adjoint
+        evaluation checks its selected
         inverses through the identity <S, Q> = dim(Q) over the BTA pattern; a
         reduced-precision point whose relative residual exceeds
         mixed_tolerance is recomputed entirely in FP64.  The residuals of the
@@ -197,8 +216,8 @@ class SpatioTemporalModel:
 
         if selinv_precision not in _PRECISIONS:
             raise ValueError(f"selinv_precision must be one of {sorted(_PRECISIONS)}")
-        if factor_precision not in ("fp64", "i8slice"):
-            raise ValueError("factor_precision must be 'fp64' or 'i8slice'")
+        if factor_precision not in ("fp64", "i8slice", "auto"):
+            raise ValueError("factor_precision must be 'fp64', 'i8slice' or 'auto'")
         self.selinv_precision = selinv_precision
         self.factor_precision = factor_precision
         self.mixed_tol = float(mixed_tolerance)
@@ -844,7 +863,7 @@ class SpatioTemporalModel:
         return self._gauss_backward(tok)
 
     def _gauss_forward(self, thetas, precision="fp64"):
-        _gauss_forward_group([(self, thetas)], self.factor_precision if precision != "fp64" else "fp64")
+        _gauss_forward_group([(self, thetas)], _factor_arith(self.factor_precision, [self], precision))
 
     def _gauss_backward(self, tok):
         return _gauss_backward_group([(self, tok)])[0]
@@ -1207,7 +1226,7 @@ def adjoint_group(jobs, precision="fp64"):
         raise NotImplementedError("grouped adjoint evaluation: Gaussian likelihoods")
     if len({id(m) for m, _ in jobs}) != len(jobs):
         raise ValueError("each model may appear once in a group")
-    fp = jobs[0][0].factor_precision if precision != "fp64" else "fp64"
+    fp = _factor_arith(jobs[0][0].factor_precision, [m for m, _ in jobs], precision)
     _gauss_forward_group(jobs, fp)
     toks = []
     for m, thetas in jobs:

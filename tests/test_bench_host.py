@@ -35,4 +35,21 @@ def test_traffic_of_another_shape_is_scaled_by_algorithmic_bytes():
 def test_default_arguments():
     a = bench.parse([])
     assert (a.workload, a.batch, a.precision, a.factor_precision, a.fd_steps) == \
-        ("gst_1500x100", 6, "i8slice", "i8slice", 3)
+        ("gst_1500x100", 6, "i8slice", "auto", 3)
+
+
+def test_auto_factor_precision_by_block_size():
+    """"auto" takes the 8-bit-slice Schur updates only when every model of the
+    group has blocks of at least AUTO_I8_FACTOR_MIN_BLOCK; an FP64 selected
+    inversion (the fallback included) always factors in FP64."""
+    from types import SimpleNamespace as NS
+
+    from dalia_b200.model import AUTO_I8_FACTOR_MIN_BLOCK as B, _factor_arith
+
+    big, small = NS(b=B), NS(b=B - 1)
+    assert _factor_arith("auto", [big], "i8slice") == "i8slice"
+    assert _factor_arith("auto", [big, small], "i8slice") == "fp64"
+    assert _factor_arith("auto", [big], "fp64") == "fp64"
+    assert _factor_arith("i8slice", [small], "i8slice") == "i8slice"
+    assert _factor_arith("i8slice", [big], "fp64") == "fp64"
+    assert _factor_arith("fp64", [big], "i8slice") == "fp64"
