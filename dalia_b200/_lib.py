@@ -71,7 +71,7 @@ SIGNATURES = {
     "bta_prof_mask": (_int, [_int]),
     "bta_prof_read": (_int, [_pdbl, ctypes.POINTER(ctypes.c_longlong)]),
     "bta_panel_task_list": (_int, [_int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _int, ctypes.POINTER(_int)]),
-    "bta_panel_task_list_ex": (_int, [_int, _c_void_p, _c_void_p, _c_void_p, _int, _c_void_p, _int,
+    "bta_panel_task_list_ex": (_int, [_int, _c_void_p, _c_void_p, _c_void_p, _int, _int, _c_void_p, _int,
                                       ctypes.POINTER(_int)]),
     "bta_tune_report": (_int, [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "bta_tune_pending": (_int, []),

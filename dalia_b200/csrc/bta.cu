@@ -127,8 +127,9 @@ struct PanelSpec {
 
 // Cached device task list of a panel batch with the given instance shapes
 // and queue lookahead.
-int get_tasks(bta_context* h, const std::vector<PanelInst>& insts, int lookahead, const int4** out, int* count) {
-  std::vector<int> key{lookahead};
+int get_tasks(bta_context* h, const std::vector<PanelInst>& insts, int lookahead, int order, const int4** out,
+              int* count) {
+  std::vector<int> key{lookahead, order};
   for (const auto& I : insts) {
     key.push_back(I.b);
     key.push_back(I.a);
@@ -138,7 +139,7 @@ int get_tasks(bta_context* h, const std::vector<PanelInst>& insts, int lookahead
   auto it = h->tasks.find(key);
   if (it == h->tasks.end()) {
     std::vector<int4> t;
-    panel_tasks(insts, t, lookahead);
+    panel_tasks(insts, t, lookahead, order);
     int4* d = nullptr;
     if (!t.empty()) {
       if (cudaMalloc(&d, t.size() * sizeof(int4)) != cudaSuccess) return BTA_ERR_ALLOC;
@@ -191,7 +192,8 @@ int run_panels(bta_context* h, const std::vector<PanelSpec>& specs, Carve& cv) {
       off += (size_t)3 * I.nrows_t * I.nq;
     }
     // launch shape: instances, their block and arrow sizes, which terms the
-    // launch applies; candidates: queue lookahead x resident CTAs per SM
+    // launch applies; candidates: resident CTAs per SM x queue order x
+    // lookahead of the previous-column terms (when the launch has them)
     std::vector<long long> tkey{(long long)insts.size()};
     for (const auto& I : insts)
       tkey.push_back(((long long)I.b << 20) | ((long long)I.a << 4) | (I.L ? 1 : 0) | (I.Lprev ? 2 : 0) |
@@ -199,17 +201,24 @@ int run_panels(bta_context* h, const std::vector<PanelSpec>& specs, Carve& cv) {
     const int occ = panel_ctas_per_sm();
     if (occ < 0) return BTA_ERR_CUDA;
     static const int kLook[3] = {PREV_LOOKAHEAD, 1, 4};
+    static const int kOrder[2] = {PANEL_ORDER_CHAIN_AHEAD, PANEL_ORDER_COLUMN};
     // only the launches that repeat within one factorisation (block columns
-    // with a previous-column term and a block below) are tuned
-    bool bulk = true;
-    for (const auto& I : insts) bulk = bulk && I.L != nullptr && I.Lprev != nullptr;
-    const int ncand = bulk ? 3 * std::min(occ, 2) : 1;
+    // with a block below) are tuned
+    bool bulk = true, prev = false;
+    for (const auto& I : insts) {
+      bulk = bulk && I.L != nullptr;
+      prev = prev || I.Lprev != nullptr;
+    }
+    const int nocc = std::min(occ, 2), nlook = prev ? 3 : 1;
+    const int ncand = bulk ? nocc * 2 * nlook : 1;
     TuneLaunch tl("panel", tkey, ncand, h->stream);
-    const int lookahead = kLook[tl.choice() % 3];
-    const int grid = device_sm_count() * (occ - tl.choice() / 3);
+    const int c = tl.choice();
+    const int grid = device_sm_count() * (occ - c % nocc);
+    const int order = kOrder[(c / nocc) % 2];
+    const int lookahead = kLook[c / (2 * nocc)];
     const int4* tasks;
     int ntasks;
-    int rc = get_tasks(h, insts, lookahead, &tasks, &ntasks);
+    int rc = get_tasks(h, insts, lookahead, order, &tasks, &ntasks);
     if (rc) return rc;
     if (cudaMemsetAsync(cnt, 0, (cnt_total + 4) * sizeof(int), h->stream) != cudaSuccess) return BTA_ERR_CUDA;
     B.ninst = (int)insts.size();
@@ -732,13 +741,13 @@ int bta_pobtasi(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, doub
 }
 
 int bta_panel_task_list(int count, const int* b, const int* a, const int* flags, int* out, int cap, int* n_out) {
-  return bta_panel_task_list_ex(count, b, a, flags, PREV_LOOKAHEAD, out, cap, n_out);
+  return bta_panel_task_list_ex(count, b, a, flags, PREV_LOOKAHEAD, PANEL_ORDER_COLUMN, out, cap, n_out);
 }
 
-int bta_panel_task_list_ex(int count, const int* b, const int* a, const int* flags, int lookahead, int* out, int cap,
-                           int* n_out) {
+int bta_panel_task_list_ex(int count, const int* b, const int* a, const int* flags, int lookahead, int order,
+                           int* out, int cap, int* n_out) {
   if (count < 1 || count > PANEL_MAXI || !b || !a || !flags || !n_out || cap < 0 || (cap > 0 && !out) ||
-      lookahead < 1)
+      lookahead < 1 || (order != PANEL_ORDER_COLUMN && order != PANEL_ORDER_CHAIN_AHEAD))
     return BTA_ERR_INVALID;
   static double present;  // stands for a matrix block: only null / non-null matters here
   std::vector<PanelInst> insts;
@@ -758,7 +767,7 @@ int bta_panel_task_list_ex(int count, const int* b, const int* a, const int* fla
     insts.push_back(I);
   }
   std::vector<int4> t;
-  panel_tasks(insts, t, lookahead);
+  panel_tasks(insts, t, lookahead, order);
   *n_out = (int)t.size();
   if ((int)t.size() > cap) return BTA_ERR_INVALID;
   for (size_t i = 0; i < t.size(); ++i) {

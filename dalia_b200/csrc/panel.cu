@@ -12,7 +12,7 @@ namespace {
 using namespace tile;
 
 #ifdef BTA_TRACE
-// Compile-time task tracer: per event {kind, p, r|q, smid, t_claim, t_ready, t_done}.
+// Compile-time task tracer: per event {kind, instance, p, r|q, smid, t_claim, t_ready, t_done}.
 __device__ unsigned long long* g_trace = nullptr;
 __device__ int g_trace_n = 0;
 __device__ __forceinline__ unsigned long long gtime() {
@@ -20,25 +20,27 @@ __device__ __forceinline__ unsigned long long gtime() {
   asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
   return t;
 }
-__device__ __forceinline__ void trace(int kind, int p, int rq, unsigned long long t0, unsigned long long t1) {
+__device__ __forceinline__ void trace(int kind, int inst, int p, int rq, unsigned long long t0,
+                                      unsigned long long t1) {
   if (threadIdx.x != 0 || g_trace == nullptr) return;
   const int i = atomicAdd(&g_trace_n, 1);
   if (i >= (1 << 20)) return;
   unsigned smid;
   asm volatile("mov.u32 %0, %smid;" : "=r"(smid));
   unsigned long long* e = g_trace + (size_t)i * 4;
-  e[0] = ((unsigned long long)kind << 56) | ((unsigned long long)p << 40) | ((unsigned long long)rq << 16) | smid;
+  e[0] = ((unsigned long long)kind << 56) | ((unsigned long long)(inst & 0xff) << 48) |
+         ((unsigned long long)(p & 0xff) << 40) | ((unsigned long long)(rq & 0xffffff) << 16) | smid;
   e[1] = t0;
   e[2] = t1;
   e[3] = gtime();
 }
 #define TRACE_T0() unsigned long long _t0 = gtime()
 #define TRACE_T1() unsigned long long _t1 = gtime()
-#define TRACE(kind, p, rq) trace(kind, p, rq, _t0, _t1)
+#define TRACE(kind, inst, p, rq) trace(kind, inst, p, rq, _t0, _t1)
 #else
 #define TRACE_T0()
 #define TRACE_T1()
-#define TRACE(kind, p, rq)
+#define TRACE(kind, inst, p, rq)
 #endif
 
 constexpr size_t SMEM_BYTES = size_t(2) * T * SG * sizeof(double);
@@ -227,13 +229,45 @@ __device__ __forceinline__ void release(int* p, int v) {
   }
 }
 
+// acc -= the tile at p (rows x cols valid, zero elsewhere), element for
+// element in the accumulator layout: acc becomes acc - A, i.e. the caller
+// negates.  All loads are issued before any use, so a read-modify-write of
+// the tile costs one L2 round trip instead of one per element (a store
+// between two loads would otherwise keep them in order).
+__device__ __forceinline__ void frag_rsub(const double* p, int ld, int rows, int cols, double (&acc)[2][4][4], int wm,
+                                          int wn, int g, int t) {
+  double v[2][2][4][2];
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int row = wm * 32 + mi * 16 + g + h * 8;
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int col = wn * 32 + ni * 8 + 2 * t + e;
+          v[mi][h][ni][e] = (row < rows && col < cols) ? __ldcg(p + (size_t)row * ld + col) : 0.0;
+        }
+    }
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) acc[mi][ni][h * 2 + e] = v[mi][h][ni][e] - acc[mi][ni][h * 2 + e];
+}
+
 // The critical path of one instance: for q = 0..nq-1,
 //   X = A(q, q-1) Linv_{q-1}^T;  A(q, q) -= X X^T;  POTRF(q);  Linv_q.
 // The two smem buffers swap roles every step: Lv holds Linv_{q-1}, Wk is work.
-__device__ void run_chain(const PanelInst& I, double* bufA, double* bufL, double* rd, int* abort_flag,
+__device__ void run_chain(const PanelInst& I, int inst, double* bufA, double* bufL, double* rd, int* abort_flag,
                           int* s_ok) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t = lane & 3;
+  (void)inst;  // read by the compile-time tracer only
   const int nq = I.nq, ld = I.b;
   double* Lv = bufL;
   double* Wk = bufA;
@@ -270,10 +304,11 @@ __device__ void run_chain(const PanelInst& I, double* bufA, double* bufL, double
       release(&I.flag[q * nq + q - 1], 1);
       if (!block_wait(&I.upd[q * nq + q], 1, abort_flag, s_ok)) return;
       TRACE_T1();
-      TRACE(8, q, 0);
+      TRACE(8, inst, q, 0);
       zero_acc(acc);
       mma_nt(Wk, Wk, T, acc, wm, wn, g, t);
       // Lv (previous inverse) is dead: it becomes the Cholesky buffer
+      frag_rsub(d.ptr, ld, w, w, acc, wm, wn, g, t);
 #pragma unroll
       for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -282,12 +317,7 @@ __device__ void run_chain(const PanelInst& I, double* bufA, double* bufL, double
 #pragma unroll
           for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
-            for (int e = 0; e < 2; ++e) {
-              const int col = wn * 32 + ni * 8 + 2 * t + e;
-              double v = 0.0;
-              if (row < w && col < w) v = __ldcg(d.ptr + (size_t)row * ld + col) - acc[mi][ni][h * 2 + e];
-              Lv[row * SG + col] = v;
-            }
+            for (int e = 0; e < 2; ++e) Lv[row * SG + wn * 32 + ni * 8 + 2 * t + e] = acc[mi][ni][h * 2 + e];
         }
       __syncthreads();
     } else {
@@ -300,7 +330,7 @@ __device__ void run_chain(const PanelInst& I, double* bufA, double* bufL, double
       potrf(Lv, rd, w, I.info, I.pivot_base + (long long)q * T, tid);
       TRACE_T1();
       trinv(Lv, Wk, rd, tid);
-      TRACE(9, q, 0);
+      TRACE(9, inst, q, 0);
     }
     double* linv = I.Linv + (size_t)q * T * T;
     for (int idx = tid; idx < T * T; idx += THREADS) {
@@ -319,8 +349,9 @@ __device__ void run_chain(const PanelInst& I, double* bufA, double* bufL, double
 }
 
 // Writes tile -= acc over its valid rows x cols (L2 reads: other CTAs wrote it).
-__device__ __forceinline__ void sub_acc(const TileRef& c, int ld, const double (&acc)[2][4][4], int wm, int wn, int g,
+__device__ __forceinline__ void sub_acc(const TileRef& c, int ld, double (&acc)[2][4][4], int wm, int wn, int g,
                                         int t) {
+  frag_rsub(c.ptr, ld, c.rows, c.cols, acc, wm, wn, g, t);
 #pragma unroll
   for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -332,10 +363,7 @@ __device__ __forceinline__ void sub_acc(const TileRef& c, int ld, const double (
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
           const int col = wn * 32 + ni * 8 + 2 * t + e;
-          if (col < c.cols) {
-            double* dst = c.ptr + (size_t)row * ld + col;
-            *dst = __ldcg(dst) - acc[mi][ni][h * 2 + e];
-          }
+          if (col < c.cols) c.ptr[(size_t)row * ld + col] = acc[mi][ni][h * 2 + e];
         }
     }
 }
@@ -353,7 +381,7 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
   if (tid == 0) s_task = atomicAdd(&B.counter[1], 1);
   __syncthreads();
   if (s_task < B.ninst) {
-    run_chain(B.inst[s_task], bufA, bufL, rd, B.abort_flag, &s_ok);
+    run_chain(B.inst[s_task], s_task, bufA, bufL, rd, B.abort_flag, &s_ok);
     return;
   }
 
@@ -378,7 +406,7 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
       TRACE_T1();
       sub_acc(tile_of(I, p, r), ld, acc, wm, wn, g, t);
       release(&I.prv[p * nq + r], 1);
-      TRACE(kind, p, r);
+      TRACE(kind, tk.x, p, r);
       continue;
     }
     if (kind == TASK_TIP) {
@@ -431,7 +459,7 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
       // chain input: write the accumulated tile, the chain CTA finishes it
       sub_acc(c, ld, acc, wm, wn, g, t);
       release(&I.upd[p * nq + r], 1);
-      TRACE(kind, p, r);
+      TRACE(kind, tk.x, p, r);
       continue;
     }
     // X(p, r) = (A(p, r) - acc) Linv_r^T
@@ -440,6 +468,7 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
     if (!s_ok) continue;
     load_async<SG>(bufL, I.Linv + (size_t)r * T * T, T, T, T, tid);
     cp_async_commit();
+    frag_rsub(c.ptr, ld, c.rows, c.cols, acc, wm, wn, g, t);
 #pragma unroll
     for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -448,12 +477,7 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
 #pragma unroll
         for (int ni = 0; ni < 4; ++ni)
 #pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            const int col = wn * 32 + ni * 8 + 2 * t + e;
-            double v = 0.0;
-            if (row < c.rows && col < c.cols) v = __ldcg(c.ptr + (size_t)row * ld + col) - acc[mi][ni][h * 2 + e];
-            bufA[row * SG + col] = v;
-          }
+          for (int e = 0; e < 2; ++e) bufA[row * SG + wn * 32 + ni * 8 + 2 * t + e] = acc[mi][ni][h * 2 + e];
       }
     cp_async_wait<0>();
     __syncthreads();
@@ -474,7 +498,7 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
           }
       }
     release(&I.flag[p * nq + r], 1);
-    TRACE(kind, p, r);
+    TRACE(kind, tk.x, p, r);
   }
 }
 
@@ -522,29 +546,96 @@ void prev_tasks(const std::vector<PanelInst>& insts, int c, std::vector<int4>& t
 
 }  // namespace
 
-void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks, int lookahead) {
+void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks, int lookahead, int order) {
   lookahead = std::max(1, lookahead);
   int max_nq = 0;
   for (const auto& I : insts) max_nq = std::max(max_nq, I.nq);
-  int prev_done = -1;  // last column whose previous-column tasks are queued
-  for (int r = 0; r < max_nq; ++r) {
-    if (prev_done < r) prev_tasks(insts, ++prev_done, tasks);
+  if (order == PANEL_ORDER_CHAIN_AHEAD) {
+    // Critical tasks first: chain step q consumes tiles (q, q-1) and (q, q),
+    // whose accumulations read rows q-1 and q of the columns up to q-2; of
+    // those, only tile (q, q-2) is a queue task that needs the chain's
+    // inverse of column q-2.  So at column r the queue holds, for every
+    // instance, the solve of tile (r+2, r) and then the chain inputs of step
+    // r+2, ahead of the bulk of column r's solves; the chain runs up to two
+    // steps ahead of the bulk instead of waiting behind it.  The
+    // previous-column terms of the chain-input tiles come before them, the
+    // rest of a column's terms `lookahead` columns ahead of its solves.
+    int crit_done = -1, bulk_done = -1;
+    auto crit_upto = [&](int c) {
+      for (c = std::min(c, max_nq - 1); crit_done < c;) {
+        ++crit_done;
+        for (int ii = 0; ii < (int)insts.size(); ++ii) {
+          const PanelInst& I = insts[ii];
+          if (crit_done >= I.nq || I.Lprev == nullptr) continue;
+          for (int p = crit_done; p < std::min(crit_done + 2, I.nq); ++p)
+            tasks.push_back(make_int4(ii, TASK_PREV, p, crit_done));
+        }
+      }
+    };
+    auto bulk_upto = [&](int c) {
+      for (c = std::min(c, max_nq - 1); bulk_done < c;) {
+        ++bulk_done;
+        crit_upto(bulk_done);
+        for (int ii = 0; ii < (int)insts.size(); ++ii) {
+          const PanelInst& I = insts[ii];
+          if (bulk_done >= I.nq || I.Lprev == nullptr) continue;
+          for (int p = std::min(bulk_done + 2, I.nq); p < I.nrows_t; ++p)
+            if (host_has_prev(I, p)) tasks.push_back(make_int4(ii, TASK_PREV, p, bulk_done));
+        }
+      }
+    };
+    crit_upto(1);
     for (int ii = 0; ii < (int)insts.size(); ++ii) {
       const PanelInst& I = insts[ii];
-      if (r >= I.nq) continue;
-      tasks.push_back(make_int4(ii, TASK_AGG_DIAG, r, r));
-      if (r + 1 < I.nq) tasks.push_back(make_int4(ii, TASK_AGG_SUB, r + 1, r));
+      tasks.push_back(make_int4(ii, TASK_AGG_DIAG, 0, 0));
+      if (I.nq > 1) {
+        tasks.push_back(make_int4(ii, TASK_AGG_SUB, 1, 0));
+        tasks.push_back(make_int4(ii, TASK_AGG_DIAG, 1, 1));
+      }
     }
-    while (prev_done < std::min(r + lookahead, max_nq - 1)) prev_tasks(insts, ++prev_done, tasks);
-    for (int ii = 0; ii < (int)insts.size(); ++ii) {
-      const PanelInst& I = insts[ii];
-      if (r >= I.nq) continue;
-      for (int p = r + 2; p < I.nq; ++p) tasks.push_back(make_int4(ii, TASK_AGG_TRSM, p, r));
+    for (int r = 0; r < max_nq; ++r) {
+      bulk_upto(r);
+      for (int ii = 0; ii < (int)insts.size(); ++ii)
+        if (r + 2 < insts[ii].nq) tasks.push_back(make_int4(ii, TASK_AGG_TRSM, r + 2, r));
+      crit_upto(r + 2);
+      for (int ii = 0; ii < (int)insts.size(); ++ii) {
+        if (r + 2 >= insts[ii].nq) continue;
+        tasks.push_back(make_int4(ii, TASK_AGG_SUB, r + 2, r + 1));
+        tasks.push_back(make_int4(ii, TASK_AGG_DIAG, r + 2, r + 2));
+      }
+      bulk_upto(r + lookahead);
+      for (int ii = 0; ii < (int)insts.size(); ++ii) {
+        const PanelInst& I = insts[ii];
+        if (r >= I.nq) continue;
+        for (int p = r + 3; p < I.nq; ++p) tasks.push_back(make_int4(ii, TASK_AGG_TRSM, p, r));
+      }
+      for (int ii = 0; ii < (int)insts.size(); ++ii) {
+        const PanelInst& I = insts[ii];
+        if (r >= I.nq) continue;
+        for (int p = std::max(I.nq, r + 1); p < I.nrows_t; ++p) tasks.push_back(make_int4(ii, TASK_AGG_TRSM, p, r));
+      }
     }
-    for (int ii = 0; ii < (int)insts.size(); ++ii) {
-      const PanelInst& I = insts[ii];
-      if (r >= I.nq) continue;
-      for (int p = std::max(I.nq, r + 1); p < I.nrows_t; ++p) tasks.push_back(make_int4(ii, TASK_AGG_TRSM, p, r));
+  } else {
+    int prev_done = -1;  // last column whose previous-column tasks are queued
+    for (int r = 0; r < max_nq; ++r) {
+      if (prev_done < r) prev_tasks(insts, ++prev_done, tasks);
+      for (int ii = 0; ii < (int)insts.size(); ++ii) {
+        const PanelInst& I = insts[ii];
+        if (r >= I.nq) continue;
+        tasks.push_back(make_int4(ii, TASK_AGG_DIAG, r, r));
+        if (r + 1 < I.nq) tasks.push_back(make_int4(ii, TASK_AGG_SUB, r + 1, r));
+      }
+      while (prev_done < std::min(r + lookahead, max_nq - 1)) prev_tasks(insts, ++prev_done, tasks);
+      for (int ii = 0; ii < (int)insts.size(); ++ii) {
+        const PanelInst& I = insts[ii];
+        if (r >= I.nq) continue;
+        for (int p = r + 2; p < I.nq; ++p) tasks.push_back(make_int4(ii, TASK_AGG_TRSM, p, r));
+      }
+      for (int ii = 0; ii < (int)insts.size(); ++ii) {
+        const PanelInst& I = insts[ii];
+        if (r >= I.nq) continue;
+        for (int p = std::max(I.nq, r + 1); p < I.nrows_t; ++p) tasks.push_back(make_int4(ii, TASK_AGG_TRSM, p, r));
+      }
     }
   }
   for (int ii = 0; ii < (int)insts.size(); ++ii)

@@ -71,8 +71,13 @@ inline int panel_rows(int b, int a, bool has_L) {
   return nq + (has_L ? nq : 0) + (a + 63) / 64;
 }
 
+// Queue orders: column by column (the chain's inputs of column r at its
+// head), or the chain's critical tasks two columns ahead of the bulk.
+enum : int { PANEL_ORDER_COLUMN = 0, PANEL_ORDER_CHAIN_AHEAD = 1 };
+
 // Queue tasks (every tile except those the chain finishes) of all instances.
-void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks, int lookahead = PREV_LOOKAHEAD);
+void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks, int lookahead = PREV_LOOKAHEAD,
+                 int order = PANEL_ORDER_COLUMN);
 
 // Launch one panel batch.  The counters of every instance, batch.counter[0..1]
 // and the abort flag must be zero-initialised by the caller.

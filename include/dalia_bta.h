@@ -264,10 +264,14 @@ int bta_prof_read(double* ms, long long* counts);
  * needs no device.  BTA_ERR_INVALID when cap is too small.
  */
 int bta_panel_task_list(int count, const int* b, const int* a, const int* flags, int* out, int cap, int* n_out);
-/* The same with the queue lookahead the autotuner may choose (tile columns by
- * which the previous-column terms run ahead; bta_panel_task_list uses 2). */
-int bta_panel_task_list_ex(int count, const int* b, const int* a, const int* flags, int lookahead, int* out, int cap,
-                           int* n_out);
+/* The same with the queue lookahead and order the autotuner chooses from:
+ * lookahead = tile columns by which the previous-column terms run ahead
+ * (bta_panel_task_list uses 2); order 0 = column by column with the chain
+ * CTA's inputs of column r at its head (bta_panel_task_list), order 1 = the
+ * solve of tile (r+2, r) and the chain's inputs of step r+2 ahead of the
+ * rest of column r. */
+int bta_panel_task_list_ex(int count, const int* b, const int* a, const int* flags, int lookahead, int order,
+                           int* out, int cap, int* n_out);
 
 /*
  * Autotuner (no counterpart in the reference).  Launch configurations of the

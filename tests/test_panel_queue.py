@@ -45,11 +45,14 @@ class Inst:
         return bool(self.flags & HAS_ABPREV) and self.a > 0
 
 
-# queue lookaheads the autotuner chooses from (2 is the default)
+# queue lookaheads the autotuner chooses from (2 is the default), and the two
+# queue orders (0: column by column, 1: the chain's critical tasks ahead)
 LOOKAHEADS = [1, 2, 4]
+ORDERS = [0, 1]
+LOOK_ORDER = [(look, order) for look in LOOKAHEADS for order in ORDERS]
 
 
-def task_list(insts, lookahead=None):
+def task_list(insts, lookahead=None, order=0):
     lib = _lib.load()
     k = len(insts)
     b = (ctypes.c_int * k)(*[i.b for i in insts])
@@ -59,7 +62,7 @@ def task_list(insts, lookahead=None):
     if lookahead is None:
         call = lambda out, cap: lib.bta_panel_task_list(k, b, a, f, out, cap, ctypes.byref(n))  # noqa: E731
     else:
-        call = lambda out, cap: lib.bta_panel_task_list_ex(k, b, a, f, lookahead, out, cap,  # noqa: E731
+        call = lambda out, cap: lib.bta_panel_task_list_ex(k, b, a, f, lookahead, order, out, cap,  # noqa: E731
                                                             ctypes.byref(n))
     assert call(None, 0) == _lib.BTA_ERR_INVALID
     out = (ctypes.c_int * (4 * n.value))()
@@ -99,11 +102,11 @@ CASES = [
 ]
 
 
-@pytest.mark.parametrize("look", LOOKAHEADS)
+@pytest.mark.parametrize("look,order", LOOK_ORDER)
 @pytest.mark.parametrize("ci", range(len(CASES)))
-def test_queue_covers_every_tile_once(ci, look):
+def test_queue_covers_every_tile_once(ci, look, order):
     insts = CASES[ci]
-    tasks = task_list(insts, look)
+    tasks = task_list(insts, look, order)
     pos = {}
     for i, (m, kind, p, r) in enumerate(tasks):
         key = (m, "prev" if kind == PREV else ("tip" if kind == TIP else "tile"), p, r)
@@ -127,14 +130,14 @@ def test_queue_covers_every_tile_once(ci, look):
     assert len(tasks) == n_tiles + n_prev + sum(inst.tip for inst in insts)
 
 
-@pytest.mark.parametrize("look", LOOKAHEADS)
+@pytest.mark.parametrize("look,order", LOOK_ORDER)
 @pytest.mark.parametrize("ci", range(len(CASES)))
-def test_queue_is_topological(ci, look):
+def test_queue_is_topological(ci, look, order):
     """Inputs of every task are produced earlier in the queue, directly or
     through the chain (whose step q consumes the tasks of tiles (q, q-1) and
     (q, q))."""
     insts = CASES[ci]
-    tasks = task_list(insts, look)
+    tasks = task_list(insts, look, order)
     where = {}
     for i, (m, kind, p, r) in enumerate(tasks):
         out = produces(kind, p, r)
@@ -204,18 +207,31 @@ def simulate(insts, tasks, workers):
             return finished
 
 
-@pytest.mark.parametrize("look", LOOKAHEADS)
+@pytest.mark.parametrize("look,order", LOOK_ORDER)
 @pytest.mark.parametrize("ci", range(len(CASES)))
 @pytest.mark.parametrize("workers", [1, 2, 3, 7, 40, 148, 296, 437])
-def test_queue_drains_with_any_number_of_ctas(ci, workers, look):
+def test_queue_drains_with_any_number_of_ctas(ci, workers, look, order):
     insts = CASES[ci]
-    tasks = task_list(insts, look)
+    tasks = task_list(insts, look, order)
     assert simulate(insts, tasks, workers) == len(tasks)
 
 
 def test_default_lookahead_is_two():
     for insts in CASES:
-        assert task_list(insts) == task_list(insts, 2)
+        assert task_list(insts) == task_list(insts, 2, 0)
+
+
+def test_chain_ahead_order_puts_critical_tasks_first():
+    """In the chain-ahead order, the solve of tile (r+2, r) and the chain's
+    inputs of step r+2 precede every other solve of column r."""
+    insts = CASES[0]
+    tasks = task_list(insts, 2, 1)
+    pos = {(m, kind, p, r): i for i, (m, kind, p, r) in enumerate(tasks)}
+    for m, inst in enumerate(insts):
+        for r in range(inst.nq - 2):
+            crit = max(pos[(m, TRSM, r + 2, r)], pos[(m, SUB, r + 2, r + 1)], pos[(m, DIAG, r + 2, r + 2)])
+            for p in range(r + 3, inst.rows):
+                assert crit < pos[(m, TRSM, p, r)]
 
 
 def test_task_list_rejects_bad_arguments():
@@ -225,7 +241,8 @@ def test_task_list_rejects_bad_arguments():
     zero = (ctypes.c_int * 1)(0)
     assert lib.bta_panel_task_list(0, one, zero, zero, None, 0, ctypes.byref(n)) == _lib.BTA_ERR_INVALID
     assert lib.bta_panel_task_list(1, zero, zero, zero, None, 0, ctypes.byref(n)) == _lib.BTA_ERR_INVALID
-    assert lib.bta_panel_task_list_ex(1, one, zero, zero, 0, None, 0, ctypes.byref(n)) == _lib.BTA_ERR_INVALID
+    assert lib.bta_panel_task_list_ex(1, one, zero, zero, 0, 0, None, 0, ctypes.byref(n)) == _lib.BTA_ERR_INVALID
+    assert lib.bta_panel_task_list_ex(1, one, zero, zero, 2, 2, None, 0, ctypes.byref(n)) == _lib.BTA_ERR_INVALID
 
 
 def noalloc_order(b, a, has_l):
