@@ -640,8 +640,8 @@ int bta_pobtasi_batched_v(bta_handle_t h, int count, const int64_t* n, const int
     const size_t bb = (size_t)b[k] * b[k], ab = (size_t)a[k] * b[k];
     if (!V || !V[k]) chunk[k] = inverse_chunk(n[k], b[k]);
     // block inverses (tile inverses + full inverses of a chunk) only when not supplied
-    need += (chunk[k] ? align_up(chunk[k] * nq * 4096 * 8) + align_up(chunk[k] * bb * 8) : 0) + 2 * align_up(bb * 8) +
-            align_up(ab * 8 + 8) + align_up(nqa * 4096 * 8 + 8) + align_up((size_t)a[k] * a[k] * 8 + 8) + 7 * kAlign;
+    need += (chunk[k] ? align_up(chunk[k] * nq * 4096 * 8) + align_up(chunk[k] * bb * 8) : 0) + align_up(bb * 8) +
+            align_up(ab * 8 + 8) + align_up(nqa * 4096 * 8 + 8) + align_up((size_t)a[k] * a[k] * 8 + 8) + 6 * kAlign;
     maxn = std::max(maxn, n[k]);
   }
   int rc = ensure_ws(h, need);
@@ -649,7 +649,7 @@ int bta_pobtasi_batched_v(bta_handle_t h, int count, const int64_t* n, const int
   cudaStream_t s = h->stream;
   Carve cv{h->ws};
   struct W {
-    double *tinv, *Linv, *G, *S, *Ga, *tinv_t, *Wt;
+    double *tinv, *Linv, *G, *Ga, *tinv_t, *Wt;
     int64_t lo;  // first block of the chunk held in Linv (own inverses)
   };
   std::vector<W> w(count);
@@ -660,7 +660,6 @@ int bta_pobtasi_batched_v(bta_handle_t h, int count, const int64_t* n, const int
     w[k].Linv = chunk[k] ? cv.take<double>(chunk[k] * bb) : const_cast<double*>(V[k]);
     w[k].lo = chunk[k] ? n[k] : 0;
     w[k].G = cv.take<double>(bb);
-    w[k].S = cv.take<double>(bb);
     w[k].Ga = cv.take<double>(ab + 1);
     w[k].tinv_t = cv.take<double>(nqa * 4096 + 1);
     w[k].Wt = cv.take<double>((size_t)a[k] * a[k] + 1);
@@ -715,7 +714,10 @@ int bta_pobtasi_batched_v(bta_handle_t h, int count, const int64_t* n, const int
         gemm_add(q, T[k], A_, w[k].Ga, B_, A_, -1.0, GF_B_KN);
         pb.push_back(q);
       }
-      GemmProb r = gemm_prob(w[k].S, B_, B_, B_, 0.0, GC_LOWER | GC_MIRROR);
+      // Sigma_ii replaces the factor block D_i in place: nothing in this
+      // step reads D_i (its inverse V_i is held apart), later steps read
+      // only blocks above it
+      GemmProb r = gemm_prob(D[k] + i * bb, B_, B_, B_, 0.0, GC_LOWER | GC_MIRROR);
       gemm_add(r, Vi, B_, Vi, B_, B_, 1.0, GF_A_T | GF_B_KN | GF_K_GE_M | GF_K_GE_N);
       if (hasL) gemm_add(r, w[k].G, B_, Li, B_, B_, -1.0, GF_A_T | GF_B_KN);
       if (a[k] > 0) gemm_add(r, w[k].Ga, B_, Abi, B_, A_, -1.0, GF_A_T | GF_B_KN);
@@ -724,13 +726,6 @@ int bta_pobtasi_batched_v(bta_handle_t h, int count, const int64_t* n, const int
     if (!pa.empty() && (rc = launch(pa))) return rc;
     if (!pb.empty() && (rc = launch(pb))) return rc;
     if (!pc.empty() && (rc = launch(pc))) return rc;
-    for (int k = 0; k < count; ++k) {
-      const int64_t i = n[k] - 1 - st;
-      if (i < 0) continue;
-      const size_t bb = (size_t)b[k] * b[k];
-      if (cudaMemcpyAsync(D[k] + i * bb, w[k].S, bb * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
-        return BTA_ERR_CUDA;
-    }
   }
   return cuda_rc(cudaGetLastError());
 }

@@ -25,9 +25,10 @@
 // digits, no multicast) into a 3-stage ring; one thread issues the products
 // of the slab, one MMA per A digit p against the stacked B digits (N up to
 // 256: 10 MMAs for 28 digit pairs), each pair (p, q) landing in the TMEM
-// accumulator of d = p + q; four epilogue warps read the OZ_S accumulators
-// (tcgen05.ld), combine them exactly, scale, release the tensor memory to
-// the next tile and write C in FP64 through a shared-memory stage.  Every
+// accumulator of d = p + q; eight epilogue warps (two per 32-lane quarter of
+// tensor memory, each taking half of the tile's columns) read the OZ_S
+// accumulators (tcgen05.ld), combine them exactly, scale, release the tensor
+// memory to the next tile and write C in FP64 through a shared-memory stage.  Every
 // wait is bounded and raises the abort flag on timeout.
 #include <algorithm>
 #include <cmath>
@@ -46,9 +47,9 @@ constexpr int QBM = 128, QBK = 32;             // output tile rows, k-slab (32 i
 constexpr int IMG = 64 * QBK;                  // one 64-row digit image (2 KB)
 constexpr int QSTAGES = 3;
 constexpr int A_SLICE = 2 * IMG;               // 128 rows
-constexpr int QTHREADS = 6 * 32;               // 4 epilogue warps, producer warp, MMA warp
-constexpr int QSTAGE_LD = 65;                  // epilogue staging: 32 rows x 64 columns per warp, padded
-constexpr int QEPI_BYTES = 4 * 32 * QSTAGE_LD * 8;
+constexpr int QEPI_WARPS = 8;                  // warps 0-7: epilogue (warp w: lanes 32 (w % 4).., column half w / 4)
+constexpr int QPROD_WARP = QEPI_WARPS, QMMA_WARP = QEPI_WARPS + 1;
+constexpr int QTHREADS = (QEPI_WARPS + 2) * 32;
 constexpr int TMEM_COLS = 512;
 constexpr long long QWAIT_CYCLES = 4000000000LL;
 constexpr int EXP_NONE = -1100;                // exponent of an all-zero row
@@ -66,7 +67,10 @@ struct QTile {
   static constexpr int STAGE_BYTES = OZ_S * (A_SLICE + B_SLICE);
   static constexpr int NSETS = BN == 32 ? 2 : 1;             // accumulator sets in tensor memory
   static constexpr int SET_COLS = 256;
-  static constexpr size_t SMEM_BYTES = size_t(QSTAGES) * STAGE_BYTES + QEPI_BYTES + 256 + 1024;
+  static constexpr int CW = BN / 2;                          // columns per epilogue warp
+  static constexpr int STAGE_LD = CW + 1;                    // its staging rows, padded
+  static constexpr int EPI_BYTES = QEPI_WARPS * 32 * STAGE_LD * 8;
+  static constexpr size_t SMEM_BYTES = size_t(QSTAGES) * STAGE_BYTES + EPI_BYTES + 256 + 1024;
   static_assert(BN == 32 || BN == 64, "tile width");
   static_assert(OZ_S * BN <= (NSETS == 2 ? SET_COLS : TMEM_COLS), "accumulators exceed tensor memory");
 };
@@ -479,7 +483,7 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   double* epi_stage = reinterpret_cast<double*>(smem + QSTAGES * TT::STAGE_BYTES);
-  uint8_t* bars = smem + QSTAGES * TT::STAGE_BYTES + QEPI_BYTES;
+  uint8_t* bars = smem + QSTAGES * TT::STAGE_BYTES + TT::EPI_BYTES;
   // barriers: full[QSTAGES], empty[QSTAGES], done[2], tmem_empty[2], drain
   const uint32_t full0 = smem_u32(bars), empty0 = full0 + 8 * QSTAGES, done0 = empty0 + 8 * QSTAGES;
   const uint32_t tmem_empty0 = done0 + 16, drain_bar = done0 + 32;
@@ -487,7 +491,7 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  if (warp == 5) {
+  if (warp == QMMA_WARP) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"((uint32_t)TMEM_COLS)
                  : "memory");
@@ -500,7 +504,7 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
     }
     for (int k = 0; k < 2; ++k) {
       mbar_init(done0 + 8 * k, 1);
-      mbar_init(tmem_empty0 + 8 * k, 4);  // one arrival per epilogue warp
+      mbar_init(tmem_empty0 + 8 * k, QEPI_WARPS);  // one arrival per epilogue warp
     }
     mbar_init(drain_bar, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -511,7 +515,7 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
   const uint32_t tmem = *tmem_slot;
   const uint32_t stage0 = smem_u32(smem);
 
-  if (warp == 4) {
+  if (warp == QPROD_WARP) {
     // ------------------------------------------------------ producer
     if (lane == 0) {
       int step = 0;
@@ -547,7 +551,7 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
         }
       }
     }
-  } else if (warp == 5) {
+  } else if (warp == QMMA_WARP) {
     // ------------------------------------------------------ MMA issuer
     if (lane == 0) {
       int step = 0, it = 0;
@@ -594,14 +598,17 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
       mbar_wait(drain_bar, 0, abort_flag);
     }
   } else {
-    // ------------------------------------------------------ epilogue (warps 0-3: rows 32 w .. 32 w + 31)
+    // ------------------------------------------------------ epilogue (warp w: rows 32 (w % 4) ..,
+    // columns (w / 4) CW .. of the tile)
     // Per 16 columns: the seven level accumulators combine exactly,
     // hi = sum_{d<4} acc_d 2^(7(3-d)) (< 2^49) and lo = sum_{d>=4} acc_d
     // 2^(7(6-d)); C = (hi + lo 2^-21) 2^(e_m + f_n - 35) goes to the warp's
     // staging rows.  Then the tensor memory is released and the warp writes
-    // whole 256-byte row segments while the next tile's products run.
-    double* stage = epi_stage + warp * (32 * QSTAGE_LD);
-    const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
+    // whole row segments while the next tile's products run.
+    constexpr int CW = TT::CW, LD = TT::STAGE_LD;
+    const int quad = warp & 3, cb = (warp >> 2) * CW;
+    double* stage = epi_stage + warp * (32 * LD);
+    const uint32_t trow = tmem + ((uint32_t)(32 * quad) << 16);
     int it = 0;
     for (int t = blockIdx.x; t < total_tiles; t += gridDim.x, ++it) {
       int pi, tm, tn;
@@ -613,64 +620,61 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
       if (!__all_sync(0xffffffffu, mbar_wait(done0 + 8 * set, use & 1, abort_flag))) break;
       tc_fence_after();
       const bool have = nsteps > 0;
-      const int row = m0 + 32 * warp + lane;
+      const int row = m0 + 32 * quad + lane;
       const bool rowok = row < P.M;
       const int er = rowok ? max(P.eA[row], EXP_NONE) : 0;
-#pragma unroll 1
-      for (int c = 0; c < BN / 32; ++c) {
-        const int col0 = n0 + 32 * c;
-        const int fcol = (col0 + lane < P.N) ? max(P.fB[col0 + lane], EXP_NONE) : 0;
-        // exponents in the normal range (every tile of ordinary data): two
-        // exact power-of-two products; otherwise ldexp on a separate path
-        const bool fast = __all_sync(0xffffffffu, er > -900 && er < 900 && fcol > -900 && fcol < 900);
-        const double srow = fast ? __longlong_as_double((long long)(er - 35 + 1023) << 52) : 0.0;
-        const double scol = fast ? __longlong_as_double((long long)(fcol + 1023) << 52) : 0.0;
+      const int col0 = n0 + cb;
+      const int fcol = (lane < CW && col0 + lane < P.N) ? max(P.fB[col0 + lane], EXP_NONE) : 0;
+      // exponents in the normal range (every tile of ordinary data): two
+      // exact power-of-two products; otherwise ldexp on a separate path
+      const bool fast = __all_sync(0xffffffffu, er > -900 && er < 900 && fcol > -900 && fcol < 900);
+      const double srow = fast ? __longlong_as_double((long long)(er - 35 + 1023) << 52) : 0.0;
+      const double scol = fast ? __longlong_as_double((long long)(fcol + 1023) << 52) : 0.0;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          long long hi[16], lo[16];
+      for (int h = 0; h < CW / 16; ++h) {
+        long long hi[16], lo[16];
 #pragma unroll
-          for (int j = 0; j < 16; ++j) hi[j] = lo[j] = 0;
-          if (have) {
-            uint32_t ra[16], rb[16];
-            const uint32_t tcol = trow + (uint32_t)(set * TT::SET_COLS + 32 * c + 16 * h);
-            tmem_ld16(tcol, ra);
+        for (int j = 0; j < 16; ++j) hi[j] = lo[j] = 0;
+        if (have) {
+          uint32_t ra[16], rb[16];
+          const uint32_t tcol = trow + (uint32_t)(set * TT::SET_COLS + cb + 16 * h);
+          tmem_ld16(tcol, ra);
 #pragma unroll
-            for (int d = 0; d < OZ_S; ++d) {
-              uint32_t cur[16];
-              if (d & 1) {
-                tmem_wait16(rb);
+          for (int d = 0; d < OZ_S; ++d) {
+            uint32_t cur[16];
+            if (d & 1) {
+              tmem_wait16(rb);
 #pragma unroll
-                for (int j = 0; j < 16; ++j) cur[j] = rb[j];
-              } else {
-                tmem_wait16(ra);
+              for (int j = 0; j < 16; ++j) cur[j] = rb[j];
+            } else {
+              tmem_wait16(ra);
 #pragma unroll
-                for (int j = 0; j < 16; ++j) cur[j] = ra[j];
-              }
-              if (d + 1 < OZ_S) {
-                if (d & 1) tmem_ld16(tcol + (uint32_t)((d + 1) * BN), ra);
-                else tmem_ld16(tcol + (uint32_t)((d + 1) * BN), rb);
-              }
+              for (int j = 0; j < 16; ++j) cur[j] = ra[j];
+            }
+            if (d + 1 < OZ_S) {
+              if (d & 1) tmem_ld16(tcol + (uint32_t)((d + 1) * BN), ra);
+              else tmem_ld16(tcol + (uint32_t)((d + 1) * BN), rb);
+            }
 #pragma unroll
-              for (int j = 0; j < 16; ++j) {
-                if (d < 4) hi[j] = hi[j] * 128 + (int)cur[j];
-                else lo[j] = lo[j] * 128 + (int)cur[j];
-              }
+            for (int j = 0; j < 16; ++j) {
+              if (d < 4) hi[j] = hi[j] * 128 + (int)cur[j];
+              else lo[j] = lo[j] * 128 + (int)cur[j];
             }
           }
-          if (fast) {
+        }
+        if (fast) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              const double sc = __shfl_sync(0xffffffffu, scol, 16 * h + j);
-              const double v = fma(exact_double(lo[j]), 0x1p-21, exact_double(hi[j]));
-              stage[lane * QSTAGE_LD + 32 * c + 16 * h + j] = ((v * srow) * sc) * P.sgn;
-            }
-          } else {
+          for (int j = 0; j < 16; ++j) {
+            const double sc = __shfl_sync(0xffffffffu, scol, 16 * h + j);
+            const double v = fma(exact_double(lo[j]), 0x1p-21, exact_double(hi[j]));
+            stage[lane * LD + 16 * h + j] = ((v * srow) * sc) * P.sgn;
+          }
+        } else {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-              const int fc = __shfl_sync(0xffffffffu, fcol, 16 * h + j);
-              const double v = fma(exact_double(lo[j]), 0x1p-21, exact_double(hi[j]));
-              stage[lane * QSTAGE_LD + 32 * c + 16 * h + j] = ldexp(v, er + fc - 35) * P.sgn;
-            }
+          for (int j = 0; j < 16; ++j) {
+            const int fc = __shfl_sync(0xffffffffu, fcol, 16 * h + j);
+            const double v = fma(exact_double(lo[j]), 0x1p-21, exact_double(hi[j]));
+            stage[lane * LD + 16 * h + j] = ldexp(v, er + fc - 35) * P.sgn;
           }
         }
       }
@@ -681,20 +685,21 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
       const bool lower = P.cflags & GC_LOWER;
       const bool mirror = P.cflags & GC_MIRROR;
       double* C = P.C;
-      const int rbase = m0 + 32 * warp;
-#pragma unroll 1
-      for (int c = 0; c < BN / 32; ++c) {
-        // row segments: lane = column
-        const int col = n0 + 32 * c + lane;
+      const int rbase = m0 + 32 * quad;
+      {
+        // row segments of CW columns: lane % CW = column, 32 / CW rows at a time
+        constexpr int RPI = 32 / CW;
+        const int cl = lane % CW, ro = lane / CW;
+        const int col = col0 + cl;
 #pragma unroll 4
-        for (int rr = 0; rr < 32; ++rr) {
+        for (int rr = ro; rr < 32; rr += RPI) {
           const int rw = rbase + rr;
           if (rw < P.M && col < P.N && (!lower || col <= rw)) {
             double* dst = C + (size_t)rw * P.ldc + col;
-            double x = stage[rr * QSTAGE_LD + 32 * c + lane];
+            double x = stage[rr * LD + cl];
             if (P.beta != 0.0) {
               x += P.beta * *dst;
-              stage[rr * QSTAGE_LD + 32 * c + lane] = x;  // the mirror copies the final value
+              stage[rr * LD + cl] = x;  // the mirror copies the final value
             }
             *dst = x;
           }
@@ -703,9 +708,9 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
         // mirror: lane = row, so the transposed writes are contiguous too
         if (mirror && rowok) {
 #pragma unroll 4
-          for (int j = 0; j < 32; ++j) {
-            const int cm = n0 + 32 * c + j;
-            if (cm < row && cm < P.N) C[(size_t)cm * P.ldc + row] = stage[lane * QSTAGE_LD + 32 * c + j];
+          for (int j = 0; j < CW; ++j) {
+            const int cm = col0 + j;
+            if (cm < row && cm < P.N) C[(size_t)cm * P.ldc + row] = stage[lane * LD + j];
           }
         }
       }
@@ -714,7 +719,7 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 5) {
+  if (warp == QMMA_WARP) {
     tc_fence_after();
     __syncwarp();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)TMEM_COLS)

@@ -1,7 +1,8 @@
 """The online autotuner: every candidate launch configuration it chooses from
-gives the same results (the factorisation's queue lookahead and CTAs per SM,
-the persistent sweep's CTAs per SM and row segments), and a factorisation of
-a new shape records a decision after trying them."""
+gives the same results (the factorisation's CTAs per SM, queue order and
+lookahead, in both the FP64 and the split Schur-update forms; the persistent
+sweep's CTAs per SM and row segments), and a factorisation of a new shape
+records a decision after trying them."""
 import ctypes
 
 import numpy as np
@@ -13,7 +14,7 @@ from oracle import bta_ref
 pytestmark = pytest.mark.gpu
 
 
-def _factor(count, n, b, a, seed):
+def _factor(count, n, b, a, seed, precision=None):
     import torch
 
     from dalia_b200 import _lib
@@ -25,16 +26,35 @@ def _factor(count, n, b, a, seed):
     arr = lambda vals, t=ctypes.c_int64: (t * count)(*vals)  # noqa: E731
     ptrs = [(ctypes.c_void_p * count)(*[d[j].data_ptr() for d in dev]) for j in range(4)]
     info = ctypes.c_int64(-1)
-    rc = lib.bta_pobtaf_batched(h.bind_stream(), count, arr([n] * count), arr([b] * count), arr([a] * count), *ptrs,
-                                ctypes.byref(info))
+    if precision is None:
+        rc = lib.bta_pobtaf_batched(h.bind_stream(), count, arr([n] * count), arr([b] * count), arr([a] * count),
+                                    *ptrs, ctypes.byref(info))
+    else:
+        rc = lib.bta_pobtaf_batched_ex(h.bind_stream(), count, arr([n] * count), arr([b] * count),
+                                       arr([a] * count), *ptrs, ctypes.byref(info), precision)
     assert rc == 0 and info.value == 0
     return mats, dev
 
 
-@pytest.mark.parametrize("cand", range(6))
+# FP64 launches with previous-column terms: 2 CTAs-per-SM x 2 orders x 3
+# lookaheads; split-form launches (Schur updates as 8-bit-slice GEMMs): 2 x 2
+@pytest.mark.parametrize("cand", range(12))
 def test_every_panel_candidate_factors_exactly(cand, monkeypatch):
     monkeypatch.setenv("DALIA_B200_TUNE_FORCE", f"panel={cand}")
     mats, dev = _factor(3, 6, 200, 5, 100 + cand)
+    for m, d in zip(mats, dev):
+        ref = [x.copy() for x in m]
+        bta_ref.pobtaf(*ref)
+        for g, r in zip(d, ref):
+            assert rel(g.cpu().numpy(), r) < 1e-10
+
+
+@pytest.mark.parametrize("cand", range(4))
+def test_every_split_panel_candidate_factors(cand, monkeypatch):
+    from dalia_b200 import _lib
+
+    monkeypatch.setenv("DALIA_B200_TUNE_FORCE", f"panel={cand}")
+    mats, dev = _factor(3, 6, 200, 5, 200 + cand, precision=_lib.BTA_PREC_I8SLICE)
     for m, d in zip(mats, dev):
         ref = [x.copy() for x in m]
         bta_ref.pobtaf(*ref)
