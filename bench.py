@@ -446,11 +446,12 @@ def run_ours(args):
     barrier()
     e0, e1 = torch.cuda.Event(True), torch.cuda.Event(True)
     e0.record()
-    fallbacks = 0
+    fallbacks = demoted = 0
     resid_max = 0.0
     for s in range(args.steps):
         run_step(nwarm + s)
         fallbacks += sum(1 for c in checks() if c["fallback"])
+        demoted += sum(1 for c in checks() if c.get("demoted"))
         resid_max = max([resid_max] + [max(c["residual_c"], c["residual_p"]) for c in checks()])
     e1.record()
     barrier()
@@ -489,7 +490,8 @@ def run_ours(args):
 
     # ---- accuracy of the reduced-precision selected inversion against FP64,
     # per result, at one point of the first member (outside every timed region)
-    accuracy = {"fallbacks_in_timed_region": fallbacks, "max_identity_residual": resid_max}
+    accuracy = {"fallbacks_in_timed_region": fallbacks, "fp64_after_failed_check_in_timed_region": demoted,
+                "max_identity_residual": resid_max}
     if args.precision != "fp64":
         sl = model.slots[0]
 

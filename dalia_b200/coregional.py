@@ -102,7 +102,7 @@ class CoregionalModel(SpatioTemporalModel):
     alpha, u)} for every key of ``prob.theta_keys``."""
 
     def __init__(self, prob, priors=None, fe_prec=1e-3, eps_gradient_f=1e-3, device=None,
-                 selinv_precision="fp64", mixed_tolerance=1e-8, factor_precision="fp64"):
+                 selinv_precision="fp64", mixed_tolerance=1e-8, factor_precision="fp64", mixed_retry=16):
         nv, ns, nt, nb = int(prob.nv), int(prob.ns), int(prob.nt), int(prob.nb)
         blocks = [sps.hstack([prob.a_st[v], sps.csc_matrix(prob.a_fe[v])], format="csc") for v in range(nv)]
         A = sps.block_diag(blocks, format="csc")[:, latent_permutation(nt, ns, nv, nb)].tocsc()
@@ -116,7 +116,7 @@ class CoregionalModel(SpatioTemporalModel):
         self.sigma_st = np.asarray(prob.sigma_st, dtype=np.float64)
         super().__init__(joint, priors={}, fe_prec=fe_prec, eps_gradient_f=eps_gradient_f, device=device,
                          selinv_precision=selinv_precision, mixed_tolerance=mixed_tolerance,
-                         factor_precision=factor_precision)
+                         factor_precision=factor_precision, mixed_retry=mixed_retry)
         self.theta_keys = list(prob.theta_keys)
         self.priors = default_priors(prob) if priors is None else dict(priors)
         missing = [k for k in self.theta_keys if k not in self.priors]

@@ -195,7 +195,7 @@ class SpatioTemporalModel:
 
     def __init__(self, prob, priors=None, fe_prec=1e-3, eps_gradient_f=1e-3, eps_inner_iteration=1e-3,
                  inner_iteration_max_iter=50, device=None, selinv_precision="fp64", mixed_tolerance=1e-8,
-                 factor_precision="fp64"):
+                 factor_precision="fp64", mixed_retry=16):
         """selinv_precision: arithmetic of the selected inversions behind the
         adjoint gradient: "fp64", "tf32x3" (FP32-class block products on the
         tcgen05 tensor cores) or "i8slice" (8-bit digit products accumulated
@@ -210,8 +210,14 @@ class SpatioTemporalModel:
         evaluation checks its selected
         inverses through the identity <S, Q> = dim(Q) over the BTA pattern; a
         reduced-precision point whose relative residual exceeds
-        mixed_tolerance is recomputed entirely in FP64.  The residuals of the
-        last evaluation are in ``last_check``."""
+        mixed_tolerance is recomputed entirely in FP64.  After such a
+        recomputation in an evaluation at the model's own precision, the next
+        mixed_retry evaluations at the model's precision run in FP64 directly
+        (the check failing again would cost the reduced-precision pass each
+        time); then the reduced precision is tried again.  An explicit
+        ``precision=`` argument is always honoured.  The residuals of the last
+        evaluation are in ``last_check`` (``demoted`` marks points run in FP64
+        by this rule)."""
         import torch
 
         if selinv_precision not in _PRECISIONS:
@@ -221,6 +227,8 @@ class SpatioTemporalModel:
         self.selinv_precision = selinv_precision
         self.factor_precision = factor_precision
         self.mixed_tol = float(mixed_tolerance)
+        self.mixed_retry = int(mixed_retry)
+        self._demote_left = 0
         self.last_check = []
 
         self.h = _lib.handle(device)
@@ -773,13 +781,20 @@ class SpatioTemporalModel:
         rp = abs(float(np.sum(cf * Ip)) - nst) / nst
         return rc, rp
 
-    def _mixed_fallback(self, thetas, fs, grads, precision):
-        """Recompute in FP64 the points whose selected-inverse check missed."""
+    def _mixed_fallback(self, thetas, fs, grads, precision, tok=None):
+        """Recompute in FP64 the points whose selected-inverse check missed
+        (and, for an evaluation at the model's own precision, run the next
+        mixed_retry such evaluations in FP64 directly)."""
+        demoted = bool(tok and tok.get("demoted"))
+        if demoted:
+            self.last_check = [dict(c, demoted=True) for c in self.last_check]
         if precision == "fp64":
             return fs, grads
         bad = [j for j, c in enumerate(self.last_check) if max(c["residual_c"], c["residual_p"]) > self.mixed_tol]
         if not bad:
             return fs, grads
+        if tok is not None and tok.get("default"):
+            self._demote_left = self.mixed_retry
         checks = list(self.last_check)
         f2, g2 = self.objective_adjoint_batched([thetas[j] for j in bad], precision="fp64")
         for j, f, g, c in zip(bad, f2, g2, self.last_check):
@@ -813,16 +828,22 @@ class SpatioTemporalModel:
         and ``f_device``; check=True synchronises and raises on a matrix
         that is not positive definite.  A later forward on this model
         invalidates the token (the backward then recomputes the forward)."""
+        default = precision is None
         precision = self.selinv_precision if precision is None else precision
         if precision not in _PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
+        demoted = False
+        if default and precision != "fp64" and self._demote_left > 0:
+            self._demote_left -= 1
+            precision, demoted = "fp64", True
         thetas = [np.asarray(t, dtype=np.float64) for t in thetas]
         if not self.gaussian:
             self._poisson_forward(thetas)
         else:
             self._gauss_forward(thetas, precision)
         self._fwd_gen = getattr(self, "_fwd_gen", 0) + 1
-        tok = {"gen": self._fwd_gen, "thetas": thetas, "precision": precision, "fs": None}
+        tok = {"gen": self._fwd_gen, "thetas": thetas, "precision": precision, "fs": None, "default": default,
+               "demoted": demoted}
         self._fwd_token = tok
         if check:
             self.status()
@@ -856,7 +877,9 @@ class SpatioTemporalModel:
         token whose device state was overwritten is recomputed first.  The
         selected inversion overwrites the factors, so the token is used up."""
         if getattr(self, "_fwd_token", None) is not tok:
-            tok = self.adjoint_forward(tok["thetas"], tok["precision"], check=False)
+            redo = self.adjoint_forward(tok["thetas"], tok["precision"], check=False)
+            redo.update(default=tok.get("default", False), demoted=tok.get("demoted", False))
+            tok = redo
         self._fwd_token = None
         if not self.gaussian:
             return self._poisson_backward(tok)
@@ -868,7 +891,7 @@ class SpatioTemporalModel:
     def _gauss_backward(self, tok):
         return _gauss_backward_group([(self, tok)])[0]
 
-    def _gauss_gradients(self, thetas, precision):
+    def _gauss_gradients(self, thetas, precision, tok=None):
         """Host half of the Gaussian backward: f and the gradient of every
         point from the scalars and block contractions on the device."""
         K = len(thetas)
@@ -903,7 +926,7 @@ class SpatioTemporalModel:
             self.last_check.append({"precision": precision, "residual_c": rc, "residual_p": rp, "fallback": False})
             fs.append(float(f))
             grads.append(grad)
-        return self._mixed_fallback(thetas, fs, grads, precision)
+        return self._mixed_fallback(thetas, fs, grads, precision, tok)
 
     # --------------------------------------------------------- marginals
     def _covariance(self, theta, x_star):
@@ -1125,7 +1148,7 @@ class SpatioTemporalModel:
             self.last_check.append({"precision": precision, "residual_c": rc, "residual_p": rp, "fallback": False})
             grads.append(grad)
         fs = list(tok["fs"])
-        return self._mixed_fallback(thetas, fs, grads, precision)
+        return self._mixed_fallback(thetas, fs, grads, precision, tok)
 
 
 # ------------------------------------------------------------------ groups
@@ -1208,7 +1231,7 @@ def _gauss_backward_group(jobs):
                                               _lib.ptr(sl.Qc.buf), _lib.ptr(m.part), m.nparts,
                                               _lib.ptr(sl.vscal[3 * j:3 * j + 1])), "gather_dot")
     lead.status()
-    return [m._gauss_gradients(tok["thetas"], precision) for m, tok in jobs]
+    return [m._gauss_gradients(tok["thetas"], precision, tok) for m, tok in jobs]
 
 
 def adjoint_group(jobs, precision="fp64"):

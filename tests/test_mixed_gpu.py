@@ -153,6 +153,36 @@ def test_mixed_fallback_recomputes_in_fp64():
     assert rel(gm, g64) < 1e-10
 
 
+def test_failed_check_runs_the_next_evaluations_in_fp64():
+    """After a fallback at the model's own precision, the next mixed_retry
+    evaluations at that precision run in FP64 directly (marked demoted), then
+    the reduced precision is tried again; an explicit precision is honoured."""
+    from dalia_b200.model import SpatioTemporalModel
+
+    g = load("gst_ragged")
+    prob = problem(g)
+    th = g["theta"]
+    f64, g64 = SpatioTemporalModel(prob).objective_adjoint(th)
+    mm = SpatioTemporalModel(prob, selinv_precision="i8slice", mixed_tolerance=0.0, mixed_retry=2)
+    seen = []
+    for _ in range(4):
+        fm, gm = mm.objective_adjoint(th)
+        c = mm.last_check[0]
+        seen.append((c["precision"], c["fallback"], c.get("demoted", False)))
+        assert abs(fm - f64) < 1e-12 * abs(f64)
+        assert rel(gm, g64) < 1e-10
+    assert seen == [("i8slice", True, False), ("fp64", False, True), ("fp64", False, True),
+                    ("i8slice", True, False)]
+    mm.objective_adjoint_batched([th], precision="i8slice")  # explicit: tried although demoted
+    assert mm.last_check[0]["precision"] == "i8slice" and mm.last_check[0]["fallback"]
+    mm.mixed_retry = 0
+    mm.objective_adjoint(th)
+    assert mm.last_check[0]["precision"] == "fp64"  # the two evaluations left from the fallback above
+    mm.objective_adjoint(th)
+    mm.objective_adjoint(th)
+    assert mm.last_check[0]["precision"] == "i8slice"
+
+
 @pytest.mark.parametrize("case", GEMM_CASES)
 def test_gemm_i8slice_matches_numpy(case):
     from dalia_b200 import _lib
