@@ -28,8 +28,10 @@ def test_traffic_of_another_shape_is_scaled_by_algorithmic_bytes():
     scale = bench.panel_bytes_per_launch(4000, 6, 2) / bench.panel_bytes_per_launch(1500, 6, 6)
     assert abs(t - 2590.0e6 * scale) < 1.0
     assert "scaled" in src
-    t2, _ = bench.roofline_traffic("x", "gemm", (1500, 6, 12))
-    assert abs(t2 - 346851328.0 * 2.0) < 1.0  # twice the matrices per launch
+    t2, _ = bench.roofline_traffic("x", "gemm", (1500, 6, 24))
+    assert abs(t2 - 346851328.0 * 4.0) < 1.0  # four times the matrices per launch
+    t3, src3 = bench.roofline_traffic("x", "gemm", (1500, 6, 12))
+    assert t3 == 706.0e6 and "same launch shape" in src3
 
 
 def test_default_arguments():
