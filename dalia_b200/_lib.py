@@ -73,6 +73,8 @@ SIGNATURES = {
     "bta_panel_task_list": (_int, [_int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _int, ctypes.POINTER(_int)]),
     "bta_panel_task_list_ex": (_int, [_int, _c_void_p, _c_void_p, _c_void_p, _int, _int, _c_void_p, _int,
                                       ctypes.POINTER(_int)]),
+    "bta_panel_task_list_all": (_int, [_int, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _int, _int, _c_void_p, _int,
+                                       ctypes.POINTER(_int)]),
     "bta_tune_report": (_int, [ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "bta_tune_pending": (_int, []),
     "bta_gather_coo": (_int, [_c_void_p, _i64, _i64, _i64, _c_void_p, _c_void_p, _i64, _int,

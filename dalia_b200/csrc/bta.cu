@@ -1,6 +1,7 @@
 // Host orchestration of the BTA factorisation, solve, selected inversion and
 // log-determinant, exported through the C ABI declared in include/dalia_bta.h.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -233,6 +234,128 @@ int run_panels(bta_context* h, const std::vector<PanelSpec>& specs, Carve& cv) {
   return BTA_OK;
 }
 
+// Whether an FP64 factorisation runs as one launch (DALIA_B200_PANEL_PERSIST=1).
+// Off by default: measured on B200 it is as fast as one launch per block
+// column on the mixed b = 1200 / 600 batch and 7 % slower on the Poisson
+// b = 2500 workload (a column launch starts with its dependency-free
+// previous-column tasks; in one launch they wait for the previous column).
+bool persist_enabled() {
+  const char* e = std::getenv("DALIA_B200_PANEL_PERSIST");
+  return e && std::strcmp(e, "1") == 0;
+}
+
+// A whole FP64 factorisation -- every block column of every instance, the
+// previous column's Schur term inside the launch -- in one launch: the
+// one-column queues of columns 0, 1, ... one after the other, each column's
+// previous-column tasks waiting on the previous column's tiles, one chain CTA
+// per instance running its columns in order.  Every column keeps its own
+// tile inverses and flags.  BTA_ERR_ALLOC when that workspace cannot be had
+// (the caller then launches column by column).
+int run_factor_persist(bta_context* h, int count, const int64_t* n, const int64_t* b, const int64_t* a,
+                       double* const* D, double* const* L, double* const* Ab, double* const* T) {
+  std::vector<int> col_start(count + 1, 0), nn(count);
+  std::vector<PanelInst> shapes(count);
+  size_t cnt_ints = (size_t)count + 4, linv_bytes = 0;
+  for (int k = 0; k < count; ++k) {
+    nn[k] = (int)n[k];
+    col_start[k + 1] = col_start[k] + nn[k];
+    PanelInst S{};
+    S.b = (int)b[k];
+    S.a = (int)a[k];
+    S.nq = (S.b + 63) / 64;
+    S.Ttip = a[k] > 0 ? T[k] : nullptr;
+    shapes[k] = S;
+    for (int c = 0; c < nn[k]; ++c) {
+      cnt_ints += (size_t)3 * panel_rows(S.b, S.a, c < nn[k] - 1) * S.nq;
+      linv_bytes += align_up((size_t)S.nq * 4096 * sizeof(double));
+    }
+  }
+  const int ncols = col_start[count];
+  const size_t need = align_up((size_t)ncols * sizeof(PanelInst)) + align_up(cnt_ints * sizeof(int)) + linv_bytes +
+                      4 * kAlign;
+  int rc = ensure_ws(h, need);
+  if (rc) return rc;
+  cudaStream_t s = h->stream;
+  Carve cv{h->ws};
+  PanelInst* dcols = cv.take<PanelInst>(ncols);
+  int* cnt = cv.take<int>(cnt_ints);
+  int* tip_seq = cnt;
+  int* batch_counter = cnt + count;
+  size_t off = (size_t)count + 4;
+  std::vector<PanelInst> cols(ncols);
+  for (int k = 0; k < count; ++k) {
+    const size_t bb = (size_t)b[k] * b[k], ab = (size_t)a[k] * b[k];
+    const int B_ = (int)b[k], A_ = (int)a[k], nq = (B_ + 63) / 64;
+    for (int c = 0; c < nn[k]; ++c) {
+      const int g = col_start[k] + c;
+      const bool hasL = c < nn[k] - 1;
+      PanelInst& I = cols[g];
+      I = PanelInst{};
+      I.D = D[k] + c * bb;
+      I.L = hasL ? L[k] + c * bb : nullptr;
+      I.Ab = A_ > 0 ? Ab[k] + c * ab : nullptr;
+      I.b = B_;
+      I.a = A_;
+      I.nq = nq;
+      I.nrows_t = panel_rows(B_, A_, hasL);
+      I.info = info_ptr(h);
+      I.pivot_base = ((long long)k << 40) + (long long)c * B_;
+      I.Lprev = c > 0 ? L[k] + (c - 1) * bb : nullptr;
+      I.Abprev = (c > 0 && A_ > 0) ? Ab[k] + (c - 1) * ab : nullptr;
+      I.Ttip = A_ > 0 ? T[k] : nullptr;
+      I.Linv = cv.take<double>((size_t)nq * 4096);
+      I.upd = cnt + off;
+      I.flag = I.upd + (size_t)I.nrows_t * nq;
+      I.prv = I.flag + (size_t)I.nrows_t * nq;
+      off += (size_t)3 * I.nrows_t * nq;
+      I.prev_flag = c > 0 ? cols[g - 1].flag : nullptr;
+      I.tip_seq = I.Ttip != nullptr ? tip_seq + k : nullptr;
+      I.col = c;
+    }
+  }
+  if (cudaMemcpyAsync(dcols, cols.data(), (size_t)ncols * sizeof(PanelInst), cudaMemcpyHostToDevice, s) !=
+          cudaSuccess ||
+      cudaMemsetAsync(cnt, 0, cnt_ints * sizeof(int), s) != cudaSuccess)
+    return BTA_ERR_CUDA;
+  // launch shape and candidates as for one column: CTAs per SM x queue order x lookahead
+  std::vector<long long> tkey{(long long)count};
+  for (int k = 0; k < count; ++k) tkey.push_back(((long long)b[k] << 40) | ((long long)a[k] << 24) | n[k]);
+  const int occ = panel_ctas_per_sm();
+  if (occ < 0) return BTA_ERR_CUDA;
+  static const int kLook[3] = {PREV_LOOKAHEAD, 1, 4};
+  static const int kOrder[2] = {PANEL_ORDER_CHAIN_AHEAD, PANEL_ORDER_COLUMN};
+  const int nocc = std::min(occ, 2);
+  TuneLaunch tl("panel_all", tkey, nocc * 6, s);
+  const int ch = tl.choice();
+  const int grid = device_sm_count() * (occ - ch % nocc);
+  const int order = kOrder[(ch / nocc) % 2], lookahead = kLook[ch / (2 * nocc)];
+  std::vector<int> key{-1, lookahead, order};
+  for (int k = 0; k < count; ++k) {
+    key.push_back((int)b[k]);
+    key.push_back((int)a[k]);
+    key.push_back(nn[k]);
+  }
+  auto it = h->tasks.find(key);
+  if (it == h->tasks.end()) {
+    std::vector<int4> t;
+    panel_tasks_persist(shapes, nn, col_start, t, lookahead, order);
+    int4* d = nullptr;
+    if (cudaMalloc(&d, t.size() * sizeof(int4)) != cudaSuccess) return BTA_ERR_ALLOC;
+    if (cudaMemcpy(d, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess) return BTA_ERR_CUDA;
+    it = h->tasks.emplace(key, std::make_pair(d, (int)t.size())).first;
+  }
+  PanelBatch B;
+  std::memset(&B, 0, sizeof(B));
+  B.ninst = count;
+  B.ntasks = it->second.second;
+  B.tasks = it->second.first;
+  B.counter = batch_counter;
+  B.abort_flag = h->ctl;
+  B.cols = dcols;
+  for (int k = 0; k <= count; ++k) B.col_start[k] = col_start[k];
+  return cuda_rc(panel_launch(B, grid, s));
+}
+
 size_t panel_ws_bytes(int b, int a) {
   const int nq = (b + 63) / 64;
   const int nr = panel_rows(b, a, true);
@@ -379,9 +502,22 @@ int bta_pobtaf_batched_ex(bta_handle_t h, int count, const int64_t* n, const int
     rc = reset_status(h);
     if (rc) return rc;
   }
+  // FP64 with every arrow tip inside the panel, when enabled: the whole
+  // factorisation in one launch, unless its workspace cannot be had
+  bool persist = !split && count <= PANEL_MAXI && persist_enabled();
+  for (int k = 0; k < count; ++k) persist = persist && a[k] <= 64;
+  if (persist) {
+    rc = run_factor_persist(h, count, n, b, a, D, L, Ab, T);
+    if (rc == BTA_ERR_ALLOC) {
+      persist = false;
+      if ((rc = ensure_ws(h, std::max(need, need_tip) + 4 * kAlign))) return rc;
+    } else if (rc) {
+      return rc;
+    }
+  }
   // pivot index of instance k: k * 2^40 + global row (1-based).  Each launch
   // factors block column i and applies block column i-1's Schur update to it.
-  for (int64_t i = 0; i < maxn; ++i) {
+  for (int64_t i = 0; i < (persist ? 0 : maxn); ++i) {
     std::vector<PanelSpec> specs;
     std::vector<GemmProb> probs;
     for (int k = 0; k < count; ++k) {
@@ -733,6 +869,38 @@ int bta_pobtasi_batched_v(bta_handle_t h, int count, const int64_t* n, const int
 int bta_pobtasi(bta_handle_t h, int64_t n, int64_t b, int64_t a, double* D, double* L, double* Ab, double* T) {
   if (!h || n < 1 || b < 1 || a < 0 || !D || (n > 1 && !L) || (a > 0 && (!Ab || !T))) return BTA_ERR_INVALID;
   return bta_pobtasi_batched(h, 1, &n, &b, &a, &D, &L, &Ab, &T);
+}
+
+int bta_panel_task_list_all(int count, const int* b, const int* a, const int* flags, const int* n, int lookahead,
+                            int order, int* out, int cap, int* n_out) {
+  if (count < 1 || count > PANEL_MAXI || !b || !a || !flags || !n || !n_out || cap < 0 || (cap > 0 && !out) ||
+      lookahead < 1 || (order != PANEL_ORDER_COLUMN && order != PANEL_ORDER_CHAIN_AHEAD))
+    return BTA_ERR_INVALID;
+  static double present;  // stands for the tip: only null / non-null matters here
+  std::vector<PanelInst> shapes(count);
+  std::vector<int> nn(count), col_start(count + 1, 0);
+  for (int k = 0; k < count; ++k) {
+    if (b[k] < 1 || a[k] < 0 || a[k] > 64 || n[k] < 1) return BTA_ERR_INVALID;
+    PanelInst S{};
+    S.b = b[k];
+    S.a = a[k];
+    S.nq = (b[k] + 63) / 64;
+    S.Ttip = ((flags[k] & 8) && a[k] > 0) ? &present : nullptr;
+    shapes[k] = S;
+    nn[k] = n[k];
+    col_start[k + 1] = col_start[k] + n[k];
+  }
+  std::vector<int4> t;
+  panel_tasks_persist(shapes, nn, col_start, t, lookahead, order);
+  *n_out = (int)t.size();
+  if ((int)t.size() > cap) return BTA_ERR_INVALID;
+  for (size_t i = 0; i < t.size(); ++i) {
+    out[4 * i] = t[i].x;
+    out[4 * i + 1] = t[i].y;
+    out[4 * i + 2] = t[i].z;
+    out[4 * i + 3] = t[i].w;
+  }
+  return BTA_OK;
 }
 
 int bta_panel_task_list(int count, const int* b, const int* a, const int* flags, int* out, int cap, int* n_out) {

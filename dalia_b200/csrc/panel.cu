@@ -107,6 +107,14 @@ __device__ __forceinline__ TileRef prev_tile_of(const PanelInst& I, int p, int c
   return t;
 }
 
+// Tile row of the previous block column holding row p's previous-column
+// source: the block below it for rows of the diagonal block, its arrow rows
+// for arrow rows (the previous column always has a block below).
+__device__ __forceinline__ int prev_row(const PanelInst& I, int p) {
+  if (p < I.nq) return I.nq + p;
+  return 2 * I.nq + (p - I.nq - (I.L != nullptr ? I.nq : 0));
+}
+
 // Whether tile (p, r) receives a previous-column term (its own TASK_PREV).
 __device__ __forceinline__ bool has_prev(const PanelInst& I, int p) {
   return I.Lprev != nullptr && prev_tile_of(I, p, 0).rows > 0;
@@ -368,6 +376,9 @@ __device__ __forceinline__ void sub_acc(const TileRef& c, int ld, double (&acc)[
     }
 }
 
+// ALL: a whole factorisation in one launch (descriptors in B.cols); the
+// one-column launch reads its descriptors from the kernel parameters.
+template <bool ALL>
 __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant__ PanelBatch B) {
   extern __shared__ __align__(16) double sm[];
   double* bufA = sm;
@@ -377,11 +388,19 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t = lane & 3;
 
-  // the first CTAs to start take the chain roles (one per instance)
+  // the first CTAs to start take the chain roles (one per instance; in a
+  // whole-factorisation launch the chain runs the instance's columns in order)
   if (tid == 0) s_task = atomicAdd(&B.counter[1], 1);
   __syncthreads();
   if (s_task < B.ninst) {
-    run_chain(B.inst[s_task], s_task, bufA, bufL, rd, B.abort_flag, &s_ok);
+    if constexpr (ALL) {
+      for (int c = B.col_start[s_task]; c < B.col_start[s_task + 1]; ++c) {
+        run_chain(B.cols[c], s_task, bufA, bufL, rd, B.abort_flag, &s_ok);
+        if (ld_acquire(B.abort_flag)) break;
+      }
+    } else {
+      run_chain(B.inst[s_task], s_task, bufA, bufL, rd, B.abort_flag, &s_ok);
+    }
     return;
   }
 
@@ -392,17 +411,22 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
     const int ti = s_task;
     if (ti >= B.ntasks) break;
     const int4 tk = B.tasks[ti];
-    const PanelInst& I = B.inst[tk.x];
+    const PanelInst& I = ALL ? B.cols[tk.x] : B.inst[tk.x];
     const int kind = tk.y, p = tk.z, r = tk.w;
     const int nq = I.nq, ld = I.b;
     TRACE_T0();
     double acc[2][4][4];
     zero_acc(acc);
     if (kind == TASK_PREV) {
-      // tile(p, r) -= Xprev(p) Xprev(r)^T: that column is final before the launch
+      // tile(p, r) -= Xprev(p) Xprev(r)^T: that column is final before a
+      // one-column launch; in a whole-factorisation launch each source tile
+      // is waited for on the previous column's flags
       const TileRef xp = prev_tile_of(I, p, 0), yp = prev_tile_of(I, r, 0);
-      acc_stream(xp.ptr, xp.rows, yp.ptr, yp.rows, ld, I.b, nullptr, nullptr, B.abort_flag, &s_ok, bufA, acc, tid,
-                 wm, wn, g, t);
+      const int* gx = I.prev_flag != nullptr ? I.prev_flag + prev_row(I, p) * nq : nullptr;
+      const int* gy = I.prev_flag != nullptr ? I.prev_flag + prev_row(I, r) * nq : nullptr;
+      if (!acc_stream(xp.ptr, xp.rows, yp.ptr, yp.rows, ld, I.b, gx, gy, B.abort_flag, &s_ok, bufA, acc, tid, wm,
+                      wn, g, t))
+        continue;
       TRACE_T1();
       sub_acc(tile_of(I, p, r), ld, acc, wm, wn, g, t);
       release(&I.prv[p * nq + r], 1);
@@ -411,12 +435,14 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
     }
     if (kind == TASK_TIP) {
       // T -= sum_k X(arrow, k) X(arrow, k)^T as the arrow row becomes final
+      // (after the previous columns' tip tasks in a whole-factorisation launch)
       const int pa = I.nrows_t - 1;
       const TileRef xa = tile_of(I, pa, 0);
       const int* gate = I.flag + pa * nq;
       if (!acc_stream(xa.ptr, xa.rows, xa.ptr, xa.rows, ld, I.b, gate, gate, B.abort_flag, &s_ok, bufA, acc, tid,
                       wm, wn, g, t))
         continue;
+      if (I.tip_seq != nullptr && !block_wait(I.tip_seq, I.col, B.abort_flag, &s_ok)) continue;
 #pragma unroll
       for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -428,9 +454,13 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
 #pragma unroll
             for (int e = 0; e < 2; ++e) {
               const int col = wn * 32 + ni * 8 + 2 * t + e;
-              if (col < I.a) I.Ttip[row * I.a + col] -= acc[mi][ni][h * 2 + e];
+              if (col < I.a) {
+                double* tp = I.Ttip + row * I.a + col;  // L2: an earlier tip task of another CTA wrote it
+                __stcg(tp, __ldcg(tp) - acc[mi][ni][h * 2 + e]);
+              }
             }
         }
+      if (I.tip_seq != nullptr) release(I.tip_seq, I.col + 1);
       continue;
     }
     // zero the mirrored strictly-upper tile (r, p) of the diagonal block
@@ -642,14 +672,51 @@ void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks, 
     if (insts[ii].Ttip != nullptr) tasks.push_back(make_int4(ii, TASK_TIP, 0, 0));
 }
 
+void panel_tasks_persist(const std::vector<PanelInst>& shapes, const std::vector<int>& n,
+                         const std::vector<int>& col_start, std::vector<int4>& tasks, int lookahead, int order) {
+  static double present;  // stands for a matrix block: only null / non-null matters to the queue
+  int maxn = 0;
+  for (int v : n) maxn = std::max(maxn, v);
+  std::vector<PanelInst> insts;
+  std::vector<int> gidx;
+  std::vector<int4> col;
+  for (int c = 0; c < maxn; ++c) {
+    insts.clear();
+    gidx.clear();
+    for (size_t k = 0; k < shapes.size(); ++k) {
+      if (c >= n[k]) continue;
+      PanelInst I = shapes[k];
+      const bool hasL = c < n[k] - 1;
+      I.L = hasL ? &present : nullptr;
+      I.Ab = I.a > 0 ? &present : nullptr;
+      I.Lprev = c > 0 ? &present : nullptr;
+      I.Abprev = (c > 0 && I.a > 0) ? &present : nullptr;
+      I.nq = (I.b + 63) / 64;
+      I.nrows_t = panel_rows(I.b, I.a, hasL);
+      insts.push_back(I);
+      gidx.push_back(col_start[k] + c);
+    }
+    col.clear();
+    panel_tasks(insts, col, lookahead, order);
+    for (int4 x : col) {
+      x.x = gidx[x.x];
+      tasks.push_back(x);
+    }
+  }
+}
+
 int panel_ctas_per_sm() {
-  const int e = ensure_smem_attr(reinterpret_cast<const void*>(panel_kernel), (int)SMEM_BYTES);
+  int e = ensure_smem_attr(reinterpret_cast<const void*>(panel_kernel<false>), (int)SMEM_BYTES);
+  if (e == cudaSuccess) e = ensure_smem_attr(reinterpret_cast<const void*>(panel_kernel<true>), (int)SMEM_BYTES);
   if (e != cudaSuccess) return -e;
   // resident CTAs per SM at this shared-memory and register use (the
   // occupancy query is cheap next to a panel launch, and answers for the
   // current device)
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel, THREADS, SMEM_BYTES);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel<false>, THREADS, SMEM_BYTES);
+  int occ_all = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_all, panel_kernel<true>, THREADS, SMEM_BYTES);
+  occ = std::min(occ, occ_all);
   return std::max(1, occ);
 }
 
@@ -667,7 +734,8 @@ int panel_launch(const PanelBatch& batch, int grid, cudaStream_t stream) {
   grid = std::max(grid, batch.ninst + (batch.ntasks > 0 ? 1 : 0));
   {
     bta::ProfScope _ps(bta::PROF_PANEL, stream);
-    panel_kernel<<<grid, THREADS, SMEM_BYTES, stream>>>(batch);
+    if (batch.cols != nullptr) panel_kernel<true><<<grid, THREADS, SMEM_BYTES, stream>>>(batch);
+    else panel_kernel<false><<<grid, THREADS, SMEM_BYTES, stream>>>(batch);
   }
   return cudaGetLastError();
 }

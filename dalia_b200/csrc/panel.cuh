@@ -17,6 +17,11 @@
 // accumulating in registers as the source columns become final, then applies
 // its TRSM (or hands the tile to the chain).  Dependencies are release/acquire flags per tile; every wait is
 // bounded and sets an abort flag instead of hanging.
+// An FP64 factorisation can also run whole in one launch: the queues of all
+// block columns one after the other, each column's previous-column tasks
+// waiting on the previous column's tiles, the chain CTA of an instance
+// running its columns in order (PanelBatch::cols; off unless
+// DALIA_B200_PANEL_PERSIST=1, as it measured no faster than column launches).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -37,9 +42,17 @@ struct PanelInst {
   int* upd;      // [nrows_t * nq] chain input tile accumulated (set to 1)
   int* flag;     // [nrows_t * nq] tile final (X computed; diagonal: Linv ready)
   int* prv;      // [nrows_t * nq] previous column's update applied (when Lprev)
+  // A factorisation in one launch: the previous column's flags (its block
+  // below and arrow rows become Lprev / Abprev while this launch runs, so
+  // the previous-column tasks wait for their source tiles), and the
+  // instance's count of finished tip tasks (the tip tasks of consecutive
+  // columns update T one after the other).  nullptr in a one-column launch.
+  const int* prev_flag;
+  int* tip_seq;
   unsigned long long* info;  // min failing pivot (1-based global index)
   long long pivot_base;      // global row index of D's first row
   int b, a, nq, nrows_t;
+  int col;       // block column index (the tip tasks' order)
 };
 
 constexpr int PANEL_MAXI = 64;
@@ -51,6 +64,12 @@ struct PanelBatch {
   int* counter;       // [0] next queue task, [1] next chain role
   int* abort_flag;    // set on a timed-out wait (all later waits return)
   PanelInst inst[PANEL_MAXI];
+  // Whole factorisation in one launch (cols != nullptr): one descriptor per
+  // (instance, block column) in device memory, instance k's columns at
+  // cols[col_start[k] .. col_start[k + 1]); task x fields index cols, and
+  // chain CTA k runs its instance's columns in order.
+  const PanelInst* cols;
+  int col_start[PANEL_MAXI + 1];
 };
 
 // Queue task kinds: the left-looking accumulation into a tile that the chain
@@ -78,6 +97,14 @@ enum : int { PANEL_ORDER_COLUMN = 0, PANEL_ORDER_CHAIN_AHEAD = 1 };
 // Queue tasks (every tile except those the chain finishes) of all instances.
 void panel_tasks(const std::vector<PanelInst>& insts, std::vector<int4>& tasks, int lookahead = PREV_LOOKAHEAD,
                  int order = PANEL_ORDER_COLUMN);
+
+// Queue of a whole factorisation in one launch: the one-column queues of
+// block columns 0, 1, ... one after the other (column c holding the
+// instances with more than c columns), task x = the column's index in the
+// descriptor array (col_start[k] + c for instance k).  cols[k] describes
+// instance k's columns' shape (b, a, tip); n[k] its number of columns.
+void panel_tasks_persist(const std::vector<PanelInst>& shapes, const std::vector<int>& n,
+                         const std::vector<int>& col_start, std::vector<int4>& tasks, int lookahead, int order);
 
 // Launch one panel batch.  The counters of every instance, batch.counter[0..1]
 // and the abort flag must be zero-initialised by the caller.

@@ -272,6 +272,16 @@ int bta_panel_task_list(int count, const int* b, const int* a, const int* flags,
  * rest of column r. */
 int bta_panel_task_list_ex(int count, const int* b, const int* a, const int* flags, int lookahead, int order,
                            int* out, int cap, int* n_out);
+/* The queue of a whole FP64 factorisation in one launch (what
+ * bta_pobtaf_batched runs when every arrow is at most 64 rows and the
+ * environment variable DALIA_B200_PANEL_PERSIST is 1): the
+ * one-column queues of block columns 0, 1, ... one after the other, matrix k
+ * having n[k] block columns (flags[k] bit 3: arrow tip); task field 0 is the
+ * column's global index (matrix k's column c is sum_{j<k} n[j] + c).  In it
+ * a previous-column task waits for its source tiles of the previous column,
+ * and the tip tasks of a matrix's columns run in column order. */
+int bta_panel_task_list_all(int count, const int* b, const int* a, const int* flags, const int* n, int lookahead,
+                            int order, int* out, int cap, int* n_out);
 
 /*
  * Autotuner (no counterpart in the reference).  Launch configurations of the

@@ -163,6 +163,44 @@ def test_batched_factor_and_selinv_match_single():
                 assert rel(y.cpu().numpy(), S[j]) < TOL
 
 
+def test_whole_factorisation_launch_is_bit_identical_to_column_launches(monkeypatch):
+    """The FP64 factorisation as one launch over every block column
+    (DALIA_B200_PANEL_PERSIST=1, arrows of at most 64 rows) and as one launch per block
+    column give bit-identical factors (the same tile tasks, each summing in
+    the same order), both within 1e-10 of the oracle; instances of different
+    block and arrow sizes and block counts share the launch."""
+    import ctypes
+
+    import torch
+
+    from dalia_b200 import _lib
+
+    lib = _lib.load()
+    h = _lib.handle()
+    shapes = [(4, 130, 3), (3, 64, 0), (6, 70, 6), (1, 200, 1), (5, 200, 64)]
+    rng = np.random.default_rng(23)
+    mats = [bta_ref.random_bta(n, b, a, rng) for n, b, a in shapes]
+    k = len(shapes)
+    I64, P = ctypes.c_int64 * k, ctypes.c_void_p * k
+    outs = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("DALIA_B200_PANEL_PERSIST", mode)
+        dev = [_cuda(*m) for m in mats]
+        args = (I64(*[s[0] for s in shapes]), I64(*[s[1] for s in shapes]), I64(*[s[2] for s in shapes]),
+                *[P(*[(t[j].data_ptr() if t[j].numel() else None) for t in dev]) for j in range(4)])
+        info = ctypes.c_int64(-1)
+        assert lib.bta_pobtaf_batched(h.bind_stream(), k, *args, ctypes.byref(info)) == 0 and info.value == 0
+        torch.cuda.synchronize()
+        outs[mode] = [[x.cpu().numpy() for x in t] for t in dev]
+    for m, one, cols in zip(mats, outs["1"], outs["0"]):
+        ref = [x.copy() for x in m]
+        bta_ref.pobtaf(*ref)
+        for x, y, r in zip(one, cols, ref):
+            if x.size:
+                assert np.array_equal(x, y)
+                assert rel(x, r) < TOL
+
+
 @pytest.mark.parametrize("n,b,a", SHAPES)
 def test_block_inverse_sweeps_and_selinv(n, b, a):
     """bta_block_inverses + bta_pobtas_inv_batched (two sweeps) against a dense

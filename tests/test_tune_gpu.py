@@ -38,9 +38,12 @@ def _factor(count, n, b, a, seed, precision=None):
 
 # FP64 launches with previous-column terms: 2 CTAs-per-SM x 2 orders x 3
 # lookaheads; split-form launches (Schur updates as 8-bit-slice GEMMs): 2 x 2
+@pytest.mark.parametrize("persist", ["1", "0"])
 @pytest.mark.parametrize("cand", range(12))
-def test_every_panel_candidate_factors_exactly(cand, monkeypatch):
-    monkeypatch.setenv("DALIA_B200_TUNE_FORCE", f"panel={cand}")
+def test_every_panel_candidate_factors_exactly(cand, persist, monkeypatch):
+    # the whole factorisation in one launch ("panel_all") and column by column ("panel")
+    monkeypatch.setenv("DALIA_B200_TUNE_FORCE", f"panel={cand},panel_all={cand}")
+    monkeypatch.setenv("DALIA_B200_PANEL_PERSIST", persist)
     mats, dev = _factor(3, 6, 200, 5, 100 + cand)
     for m, d in zip(mats, dev):
         ref = [x.copy() for x in m]
@@ -82,14 +85,18 @@ def test_every_sweep_candidate_solves_exactly(cand, monkeypatch):
 
 
 def test_tuner_decides_and_reports(monkeypatch):
-    """A batched factorisation with many block columns of one new shape: the
-    tuner tries the panel candidates on its block columns and records a
-    decision, still giving the exact factor."""
+    """Launched column by column, a batched factorisation with many block
+    columns of one new shape lets the tuner try the panel candidates on its
+    block columns and record a decision; as one launch per factorisation,
+    the candidates are tried on successive factorisations of one shape
+    (12 candidates, 2 trials each).  Every factor stays exact."""
     from dalia_b200 import _lib
 
     monkeypatch.delenv("DALIA_B200_TUNE_FORCE", raising=False)
     monkeypatch.delenv("DALIA_B200_TUNE", raising=False)
-    mats, dev = _factor(2, 20, 131, 3, 300)
+    monkeypatch.setenv("DALIA_B200_PANEL_PERSIST", "0")
+    # 29 launches with a previous-column term: 12 candidates x 2 trials, then the decision
+    mats, dev = _factor(2, 30, 131, 3, 300)
     for m, d in zip(mats, dev):
         ref = [x.copy() for x in m]
         bta_ref.pobtaf(*ref)
@@ -97,3 +104,13 @@ def test_tuner_decides_and_reports(monkeypatch):
             assert rel(g.cpu().numpy(), r) < 1e-10
     lines = _lib.tune_report()
     assert any(ln.startswith("panel|") and "best=" in ln for ln in lines), lines
+    monkeypatch.setenv("DALIA_B200_PANEL_PERSIST", "1")
+    for it in range(25):
+        mats, dev = _factor(2, 4, 133, 3, 400 + it)
+        for m, d in zip(mats, dev):
+            ref = [x.copy() for x in m]
+            bta_ref.pobtaf(*ref)
+            for g, r in zip(d, ref):
+                assert rel(g.cpu().numpy(), r) < 1e-10
+    lines = _lib.tune_report()
+    assert any(ln.startswith("panel_all|") and "best=" in ln for ln in lines), lines
