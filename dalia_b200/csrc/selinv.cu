@@ -131,15 +131,18 @@ __global__ void __launch_bounds__(THREADS) block_trtri_kernel(const double* D, c
       if (r < wc && cc < wc) Oi[(size_t)(c * T + r) * b + c * T + cc] = Lc[idx];
     }
   }
-  __threadfence();
+  // the column's tiles are read back only by this CTA: a CTA barrier orders them
   __syncthreads();
   for (int p = c + 1; p < nq; ++p) {
     const int rp = min(T, b - p * T);
+    // the inverse of diagonal tile p arrives while the column sum streams
+    load_async<SG>(Ys, tile_inv + (size_t)(i * nq + p) * T * T, T, T, T, tid);
+    cp_async_commit();
     double acc[2][4][4];
     zero_acc(acc);
     // acc = L[p][c..p-1] X[c..p-1][c], streamed over k in 16-wide slabs
     trtri_stream(Di + (size_t)(p * T) * b, rp, Oi + c * T, wc, c * T, p * T, b, As, acc, tid, wm, wn, g, t);
-    // Ys[n][j] = acc[j][n]
+    // As[n][j] = acc[j][n] (the slab ring is free again)
 #pragma unroll
     for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -150,13 +153,12 @@ __global__ void __launch_bounds__(THREADS) block_trtri_kernel(const double* D, c
 #pragma unroll
           for (int e = 0; e < 2; ++e) {
             const int n = wn * 32 + ni * 8 + 2 * t + e;
-            Ys[n * SG + j] = acc[mi][ni][h * 2 + e];
+            As[n * SG + j] = acc[mi][ni][h * 2 + e];
           }
       }
-    load<SG>(As, tile_inv + (size_t)(i * nq + p) * T * T, T, T, T, tid);
     __syncthreads();
     zero_acc(acc);
-    mma_nt(As, Ys, T, acc, wm, wn, g, t);
+    mma_nt(Ys, As, T, acc, wm, wn, g, t);
 #pragma unroll
     for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -171,8 +173,7 @@ __global__ void __launch_bounds__(THREADS) block_trtri_kernel(const double* D, c
             if (n < wc) Oi[(size_t)(p * T + r) * b + c * T + n] = -acc[mi][ni][h * 2 + e];
           }
       }
-    __threadfence();
-    __syncthreads();
+    __syncthreads();  // the next step reads this tile and refills Ys
   }
 }
 
