@@ -45,7 +45,7 @@ namespace {
 constexpr int OZ_S = 7;                        // digits per operand
 constexpr int QBM = 128, QBK = 32;             // output tile rows, k-slab (32 int8 = one 32-byte row)
 constexpr int IMG = 64 * QBK;                  // one 64-row digit image (2 KB)
-constexpr int QSTAGES = 3;
+constexpr int QSTAGES = 4;
 constexpr int A_SLICE = 2 * IMG;               // 128 rows
 constexpr int QEPI_WARPS = 8;                  // warps 0-7: epilogue (warp w: lanes 32 (w % 4).., column half w / 4)
 constexpr int QPROD_WARP = QEPI_WARPS, QMMA_WARP = QEPI_WARPS + 1;
@@ -68,7 +68,7 @@ struct QTile {
   static constexpr int NSETS = BN == 32 ? 2 : 1;             // accumulator sets in tensor memory
   static constexpr int SET_COLS = 256;
   static constexpr int CW = BN / 2;                          // columns per epilogue warp
-  static constexpr int STAGE_LD = CW + 1;                    // its staging rows, padded
+  static constexpr int STAGE_LD = 17;                        // its staging rows (16 columns at a time), padded
   static constexpr int EPI_BYTES = QEPI_WARPS * 32 * STAGE_LD * 8;
   static constexpr size_t SMEM_BYTES = size_t(QSTAGES) * STAGE_BYTES + EPI_BYTES + 256 + 1024;
   static_assert(BN == 32 || BN == 64, "tile width");
@@ -603,8 +603,9 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
     // Per 16 columns: the seven level accumulators combine exactly,
     // hi = sum_{d<4} acc_d 2^(7(3-d)) (< 2^49) and lo = sum_{d>=4} acc_d
     // 2^(7(6-d)); C = (hi + lo 2^-21) 2^(e_m + f_n - 35) goes to the warp's
-    // staging rows.  Then the tensor memory is released and the warp writes
-    // whole row segments while the next tile's products run.
+    // registers.  Then the tensor memory is released and the warp writes
+    // whole 16-column row segments through its staging rows while the next
+    // tile's products run.
     constexpr int CW = TT::CW, LD = TT::STAGE_LD;
     const int quad = warp & 3, cb = (warp >> 2) * CW;
     double* stage = epi_stage + warp * (32 * LD);
@@ -630,6 +631,7 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
       const bool fast = __all_sync(0xffffffffu, er > -900 && er < 900 && fcol > -900 && fcol < 900);
       const double srow = fast ? __longlong_as_double((long long)(er - 35 + 1023) << 52) : 0.0;
       const double scol = fast ? __longlong_as_double((long long)(fcol + 1023) << 52) : 0.0;
+      double res[CW / 16][16];  // this lane's row, the warp's CW columns
 #pragma unroll
       for (int h = 0; h < CW / 16; ++h) {
         long long hi[16], lo[16];
@@ -667,14 +669,14 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
           for (int j = 0; j < 16; ++j) {
             const double sc = __shfl_sync(0xffffffffu, scol, 16 * h + j);
             const double v = fma(exact_double(lo[j]), 0x1p-21, exact_double(hi[j]));
-            stage[lane * LD + 16 * h + j] = ((v * srow) * sc) * P.sgn;
+            res[h][j] = ((v * srow) * sc) * P.sgn;
           }
         } else {
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             const int fc = __shfl_sync(0xffffffffu, fcol, 16 * h + j);
             const double v = fma(exact_double(lo[j]), 0x1p-21, exact_double(hi[j]));
-            stage[lane * LD + 16 * h + j] = ldexp(v, er + fc - 35) * P.sgn;
+            res[h][j] = ldexp(v, er + fc - 35) * P.sgn;
           }
         }
       }
@@ -686,13 +688,18 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
       const bool mirror = P.cflags & GC_MIRROR;
       double* C = P.C;
       const int rbase = m0 + 32 * quad;
-      {
-        // row segments of CW columns: lane % CW = column, 32 / CW rows at a time
-        constexpr int RPI = 32 / CW;
-        const int cl = lane % CW, ro = lane / CW;
-        const int col = col0 + cl;
+#pragma unroll
+      for (int h = 0; h < CW / 16; ++h) {
+        // 16 columns through the staging rows: lane = row to stage them,
+        // then lane % 16 = column, two rows at a time, for the stores
+#pragma unroll
+        for (int j = 0; j < 16; ++j) stage[lane * LD + j] = res[h][j];
+        __syncwarp();
+        const int c0 = col0 + 16 * h;
+        const int cl = lane & 15, ro = lane >> 4;
+        const int col = c0 + cl;
 #pragma unroll 4
-        for (int rr = ro; rr < 32; rr += RPI) {
+        for (int rr = ro; rr < 32; rr += 2) {
           const int rw = rbase + rr;
           if (rw < P.M && col < P.N && (!lower || col <= rw)) {
             double* dst = C + (size_t)rw * P.ldc + col;
@@ -708,11 +715,12 @@ __global__ void __launch_bounds__(QTHREADS, 1) gemm_i8_kernel(const __grid_const
         // mirror: lane = row, so the transposed writes are contiguous too
         if (mirror && rowok) {
 #pragma unroll 4
-          for (int j = 0; j < CW; ++j) {
-            const int cm = col0 + j;
+          for (int j = 0; j < 16; ++j) {
+            const int cm = c0 + j;
             if (cm < row && cm < P.N) C[(size_t)cm * P.ldc + row] = stage[lane * LD + j];
           }
         }
+        __syncwarp();
       }
       __syncwarp();
     }
