@@ -292,7 +292,8 @@ __device__ void run_chain(const PanelInst& I, int inst, double* bufA, double* bu
       __syncthreads();
       double acc[2][4][4];
       zero_acc(acc);
-      mma_nt(Wk, Lv, T, acc, wm, wn, g, t);
+      // Linv_{q-1} is lower triangular: output column n sums k <= n only
+      mma_nt(Wk, Lv, 32 * (wn + 1), acc, wm, wn, g, t);
       __syncthreads();
 #pragma unroll
       for (int mi = 0; mi < 2; ++mi)
@@ -512,7 +513,8 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
     cp_async_wait<0>();
     __syncthreads();
     zero_acc(acc);
-    mma_nt(bufA, bufL, (c.cols + 3) & ~3, acc, wm, wn, g, t);
+    // Linv_r is lower triangular: output column n sums k <= n only
+    mma_nt(bufA, bufL, min((c.cols + 3) & ~3, 32 * (wn + 1)), acc, wm, wn, g, t);
 #pragma unroll
     for (int mi = 0; mi < 2; ++mi)
 #pragma unroll

@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(THREADS) block_trtri_kernel(const double* D, c
       }
     __syncthreads();
     zero_acc(acc);
-    mma_nt(Ys, As, T, acc, wm, wn, g, t);
+    mma_nt(Ys, As, 32 * (wm + 1), acc, wm, wn, g, t);  // Linv_pp lower triangular: row j sums k <= j
 #pragma unroll
     for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
