@@ -216,8 +216,7 @@ int bta_gather_coo(bta_handle_t h, int64_t n, int64_t b, int64_t a, const int64_
  * holds until the process exits.  Sizes: b <= BTA_NOALLOC_MAX_B and
  * a <= BTA_NOALLOC_MAX_A (any n); larger problems are rejected with
  * BTA_ERR_INVALID before any GPU work.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress) -- make that first call
- * before any stream capture.  With info != NULL the call synchronises the
+ * the array's device address (cudaGetSymbolAddress).  With info != NULL the call synchronises the
  * stream and reports a non-positive pivot (info, BTA_ERR_NOT_SPD) or a
  * timed-out device wait (BTA_ERR_TIMEOUT).  With info == NULL it returns
  * without waiting; the status stays in the array until the next call clears
