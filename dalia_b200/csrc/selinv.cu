@@ -11,14 +11,15 @@ namespace bta {
 namespace {
 
 using namespace tile;
-constexpr size_t TRTRI_SMEM = size_t(3) * T * SG * sizeof(double);
-
 // Slab ring of the column substitution: A = 64 rows x 16 k of a row block of
 // the factor (k-contiguous, stride TSK), B = 16 k x 64 columns of the output
-// (n-contiguous, stride TSN), three stages in the As / Bs buffers.
-constexpr int TK = 16, TSK = TK + 4, TSN = T + 4, TST = 3;
+// (n-contiguous, stride TSN), two stages; three CTAs per SM hide the rest.
+constexpr int TK = 16, TSK = TK + 4, TSN = T + 4, TST = 2;
 constexpr int TA_SLAB = T * TSK, TB_SLAB = TK * TSN;
-static_assert(TST * (TA_SLAB + TB_SLAB) <= 2 * T * SG, "slab ring exceeds As + Bs");
+// shared memory: the ring (also the staging of a step's sum, 64 x SG), then
+// the diagonal tile inverse (64 x SG)
+constexpr int TRTRI_RING = TST * (TA_SLAB + TB_SLAB) > T * SG ? TST * (TA_SLAB + TB_SLAB) : T * SG;
+constexpr size_t TRTRI_SMEM = size_t(TRTRI_RING + T * SG) * sizeof(double);
 
 __device__ __forceinline__ void trtri_load(double* As, double* Bs, const double* Arow, int rows, const double* Bcol,
                                            int cols, int k0, int kend, int ld, int tid) {
@@ -103,11 +104,11 @@ __device__ void trtri_stream(const double* Arow, int rows, const double* Bcol, i
 // One CTA per (block, tile column c): forward substitution down the column,
 //   X[c] = Linv_cc,  X[p] = -Linv_pp * sum_{k=c}^{p-1} L[p][k] X[k]   (p > c).
 // blockIdx.x = c * nblk + block so that the longest columns start first.
-__global__ void __launch_bounds__(THREADS) block_trtri_kernel(const double* D, const double* tile_inv, int i0,
+__global__ void __launch_bounds__(THREADS, 3) block_trtri_kernel(const double* D, const double* tile_inv, int i0,
                                                                int nblk, int b, int nq, double* out) {
   extern __shared__ __align__(16) double sm[];
   double* As = sm;
-  double* Ys = sm + 2 * T * SG;
+  double* Ys = sm + TRTRI_RING;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t = lane & 3;
   const int c = blockIdx.x / nblk, bi = blockIdx.x % nblk, i = i0 + bi;
