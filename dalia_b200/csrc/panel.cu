@@ -342,13 +342,23 @@ __device__ void run_chain(const PanelInst& I, int inst, double* bufA, double* bu
       TRACE(9, inst, q, 0);
     }
     double* linv = I.Linv + (size_t)q * T * T;
-    for (int idx = tid; idx < T * T; idx += THREADS) {
+    // two columns per thread (16-byte accesses when the tile's rows allow)
+    const bool vec = ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(d.ptr) & 15) == 0);
+    for (int idx = 2 * tid; idx < T * T; idx += 2 * THREADS) {
       const int i = idx >> 6, k = idx & 63;
-      const bool in = i < w && k < w;
-      if (in) d.ptr[(size_t)i * ld + k] = Lv[i * SG + k];
-      const double li = in ? Wk[i * SG + k] : 0.0;
-      linv[idx] = li;
-      Wk[i * SG + k] = li;  // zero-padded operand for the next step
+      const bool in0 = i < w && k < w, in1 = i < w && k + 1 < w;
+      const double2 l = *reinterpret_cast<const double2*>(Lv + i * SG + k);
+      const double2 v = *reinterpret_cast<const double2*>(Wk + i * SG + k);
+      const double2 li = make_double2(in0 ? v.x : 0.0, in1 ? v.y : 0.0);
+      double* dp = d.ptr + (size_t)i * ld + k;
+      if (vec && in1) {
+        *reinterpret_cast<double2*>(dp) = l;
+      } else {
+        if (in0) dp[0] = l.x;
+        if (in1) dp[1] = l.y;
+      }
+      *reinterpret_cast<double2*>(linv + idx) = li;
+      *reinterpret_cast<double2*>(Wk + i * SG + k) = li;  // zero-padded operand for the next step
     }
     double* tmp = Lv;
     Lv = Wk;

@@ -135,13 +135,17 @@ __device__ __forceinline__ void potrf(double* S, double* rd, int w, unsigned lon
       double d[16];
 #pragma unroll
       for (int k = 0; k < 16; ++k) d[k] = S[(o + i) * SG + o + k];
+      // dn: lane j+1's next pivot, updated from its own l_{j+1,j} (the same
+      // fma as its column update, off the shuffle of that update's operand)
+      double dn = d[0];
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
-        const double piv = __shfl_sync(0xffffffffu, d[j], j, 16);
+        const double piv = __shfl_sync(0xffffffffu, dn, j, 16);
         if (lane == 0 && o + j < w && !(piv > 0.0) && info != nullptr)
           atomicMin(info, (unsigned long long)(base + o + j + 1));
         const double rs = rsqrt_nr(piv);
         const double lij = d[j] * rs;
+        if (j + 1 < 16) dn = fma(-lij, lij, d[j + 1]);
 #pragma unroll
         for (int k = j + 1; k < 16; ++k) {
           const double lkj = __shfl_sync(0xffffffffu, lij, k, 16);
