@@ -244,6 +244,7 @@ __device__ __forceinline__ void release(int* p, int v) {
 // between two loads would otherwise keep them in order).
 __device__ __forceinline__ void frag_rsub(const double* p, int ld, int rows, int cols, double (&acc)[2][4][4], int wm,
                                           int wn, int g, int t) {
+  const bool vec = ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(p) & 15) == 0);
   double v[2][2][4][2];
 #pragma unroll
   for (int mi = 0; mi < 2; ++mi)
@@ -251,12 +252,18 @@ __device__ __forceinline__ void frag_rsub(const double* p, int ld, int rows, int
     for (int h = 0; h < 2; ++h) {
       const int row = wm * 32 + mi * 16 + g + h * 8;
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int col = wn * 32 + ni * 8 + 2 * t + e;
-          v[mi][h][ni][e] = (row < rows && col < cols) ? __ldcg(p + (size_t)row * ld + col) : 0.0;
+      for (int ni = 0; ni < 4; ++ni) {
+        const int col = wn * 32 + ni * 8 + 2 * t;  // even: a column pair
+        const double* src = p + (size_t)row * ld + col;
+        if (vec && row < rows && col + 1 < cols) {
+          const double2 x = __ldcg(reinterpret_cast<const double2*>(src));
+          v[mi][h][ni][0] = x.x;
+          v[mi][h][ni][1] = x.y;
+        } else {
+          v[mi][h][ni][0] = (row < rows && col < cols) ? __ldcg(src) : 0.0;
+          v[mi][h][ni][1] = (row < rows && col + 1 < cols) ? __ldcg(src + 1) : 0.0;
         }
+      }
     }
 #pragma unroll
   for (int mi = 0; mi < 2; ++mi)
@@ -367,24 +374,36 @@ __device__ void run_chain(const PanelInst& I, int inst, double* bufA, double* bu
   }
 }
 
-// Writes tile -= acc over its valid rows x cols (L2 reads: other CTAs wrote it).
-__device__ __forceinline__ void sub_acc(const TileRef& c, int ld, double (&acc)[2][4][4], int wm, int wn, int g,
-                                        int t) {
-  frag_rsub(c.ptr, ld, c.rows, c.cols, acc, wm, wn, g, t);
+// Writes the accumulator tile to rows x cols of p (column pairs as 16-byte
+// stores when the rows allow).
+__device__ __forceinline__ void store_frag(double* p, int ld, int rows, int cols, const double (&acc)[2][4][4],
+                                           int wm, int wn, int g, int t) {
+  const bool vec = ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(p) & 15) == 0);
 #pragma unroll
   for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int row = wm * 32 + mi * 16 + g + h * 8;
-      if (row >= c.rows) continue;
+      if (row >= rows) continue;
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int col = wn * 32 + ni * 8 + 2 * t + e;
-          if (col < c.cols) c.ptr[(size_t)row * ld + col] = acc[mi][ni][h * 2 + e];
+      for (int ni = 0; ni < 4; ++ni) {
+        const int col = wn * 32 + ni * 8 + 2 * t;
+        double* dst = p + (size_t)row * ld + col;
+        if (vec && col + 1 < cols) {
+          *reinterpret_cast<double2*>(dst) = make_double2(acc[mi][ni][h * 2], acc[mi][ni][h * 2 + 1]);
+        } else {
+          if (col < cols) dst[0] = acc[mi][ni][h * 2];
+          if (col + 1 < cols) dst[1] = acc[mi][ni][h * 2 + 1];
         }
+      }
     }
+}
+
+// Writes tile -= acc over its valid rows x cols (L2 reads: other CTAs wrote it).
+__device__ __forceinline__ void sub_acc(const TileRef& c, int ld, double (&acc)[2][4][4], int wm, int wn, int g,
+                                        int t) {
+  frag_rsub(c.ptr, ld, c.rows, c.cols, acc, wm, wn, g, t);
+  store_frag(c.ptr, ld, c.rows, c.cols, acc, wm, wn, g, t);
 }
 
 // ALL: a whole factorisation in one launch (descriptors in B.cols); the
@@ -525,20 +544,7 @@ __global__ void __launch_bounds__(THREADS, 3) panel_kernel(const __grid_constant
     zero_acc(acc);
     // Linv_r is lower triangular: output column n sums k <= n only
     mma_nt(bufA, bufL, min((c.cols + 3) & ~3, 32 * (wn + 1)), acc, wm, wn, g, t);
-#pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int row = wm * 32 + mi * 16 + g + h * 8;
-        if (row >= c.rows) continue;
-#pragma unroll
-        for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            const int col = wn * 32 + ni * 8 + 2 * t + e;
-            if (col < c.cols) c.ptr[(size_t)row * ld + col] = acc[mi][ni][h * 2 + e];
-          }
-      }
+    store_frag(c.ptr, ld, c.rows, c.cols, acc, wm, wn, g, t);
     release(&I.flag[p * nq + r], 1);
     TRACE(kind, tk.x, p, r);
   }
