@@ -275,6 +275,31 @@ __device__ __forceinline__ void frag_rsub(const double* p, int ld, int rows, int
         for (int e = 0; e < 2; ++e) acc[mi][ni][h * 2 + e] = v[mi][h][ni][e] - acc[mi][ni][h * 2 + e];
 }
 
+// Writes the accumulator tile to rows x cols of p (column pairs as 16-byte
+// stores when the rows allow).
+__device__ __forceinline__ void store_frag(double* p, int ld, int rows, int cols, const double (&acc)[2][4][4],
+                                           int wm, int wn, int g, int t) {
+  const bool vec = ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(p) & 15) == 0);
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int row = wm * 32 + mi * 16 + g + h * 8;
+      if (row >= rows) continue;
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+        const int col = wn * 32 + ni * 8 + 2 * t;
+        double* dst = p + (size_t)row * ld + col;
+        if (vec && col + 1 < cols) {
+          *reinterpret_cast<double2*>(dst) = make_double2(acc[mi][ni][h * 2], acc[mi][ni][h * 2 + 1]);
+        } else {
+          if (col < cols) dst[0] = acc[mi][ni][h * 2];
+          if (col + 1 < cols) dst[1] = acc[mi][ni][h * 2 + 1];
+        }
+      }
+    }
+}
+
 // The critical path of one instance: for q = 0..nq-1,
 //   X = A(q, q-1) Linv_{q-1}^T;  A(q, q) -= X X^T;  POTRF(q);  Linv_q.
 // The two smem buffers swap roles every step: Lv holds Linv_{q-1}, Wk is work.
@@ -308,15 +333,14 @@ __device__ void run_chain(const PanelInst& I, int inst, double* bufA, double* bu
         for (int h = 0; h < 2; ++h) {
           const int row = wm * 32 + mi * 16 + g + h * 8;
 #pragma unroll
-          for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-              const int col = wn * 32 + ni * 8 + 2 * t + e;
-              const double v = (row < x.rows) ? acc[mi][ni][h * 2 + e] : 0.0;
-              Wk[row * SG + col] = v;
-              if (row < x.rows && col < x.cols) x.ptr[(size_t)row * ld + col] = v;
-            }
+          for (int ni = 0; ni < 4; ++ni) {
+            const int col = wn * 32 + ni * 8 + 2 * t;
+            const bool in = row < x.rows;
+            *reinterpret_cast<double2*>(Wk + row * SG + col) =
+                make_double2(in ? acc[mi][ni][h * 2] : 0.0, in ? acc[mi][ni][h * 2 + 1] : 0.0);
+          }
         }
+      store_frag(x.ptr, ld, x.rows, x.cols, acc, wm, wn, g, t);
       release(&I.flag[q * nq + q - 1], 1);
       if (!block_wait(&I.upd[q * nq + q], 1, abort_flag, s_ok)) return;
       TRACE_T1();
@@ -372,31 +396,6 @@ __device__ void run_chain(const PanelInst& I, int inst, double* bufA, double* bu
     Wk = tmp;
     release(&I.flag[q * nq + q], 1);
   }
-}
-
-// Writes the accumulator tile to rows x cols of p (column pairs as 16-byte
-// stores when the rows allow).
-__device__ __forceinline__ void store_frag(double* p, int ld, int rows, int cols, const double (&acc)[2][4][4],
-                                           int wm, int wn, int g, int t) {
-  const bool vec = ((ld & 1) == 0) && ((reinterpret_cast<uintptr_t>(p) & 15) == 0);
-#pragma unroll
-  for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int row = wm * 32 + mi * 16 + g + h * 8;
-      if (row >= rows) continue;
-#pragma unroll
-      for (int ni = 0; ni < 4; ++ni) {
-        const int col = wn * 32 + ni * 8 + 2 * t;
-        double* dst = p + (size_t)row * ld + col;
-        if (vec && col + 1 < cols) {
-          *reinterpret_cast<double2*>(dst) = make_double2(acc[mi][ni][h * 2], acc[mi][ni][h * 2 + 1]);
-        } else {
-          if (col < cols) dst[0] = acc[mi][ni][h * 2];
-          if (col + 1 < cols) dst[1] = acc[mi][ni][h * 2 + 1];
-        }
-      }
-    }
 }
 
 // Writes tile -= acc over its valid rows x cols (L2 reads: other CTAs wrote it).

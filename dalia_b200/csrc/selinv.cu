@@ -160,20 +160,30 @@ __global__ void __launch_bounds__(THREADS, 3) block_trtri_kernel(const double* D
     __syncthreads();
     zero_acc(acc);
     mma_nt(Ys, As, 32 * (wm + 1), acc, wm, wn, g, t);  // Linv_pp lower triangular: row j sums k <= j
+    {
+      // -acc to rows rp x columns wc of the output tile (column pairs as
+      // 16-byte stores when the rows allow)
+      double* o = Oi + (size_t)(p * T) * b + c * T;
+      const bool vec = ((b & 1) == 0) && ((reinterpret_cast<uintptr_t>(o) & 15) == 0);
 #pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
+      for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int r = wm * 32 + mi * 16 + g + h * 8;
-        if (r >= rp) continue;
+        for (int h = 0; h < 2; ++h) {
+          const int r = wm * 32 + mi * 16 + g + h * 8;
+          if (r >= rp) continue;
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-          for (int e = 0; e < 2; ++e) {
-            const int n = wn * 32 + ni * 8 + 2 * t + e;
-            if (n < wc) Oi[(size_t)(p * T + r) * b + c * T + n] = -acc[mi][ni][h * 2 + e];
+          for (int ni = 0; ni < 4; ++ni) {
+            const int n = wn * 32 + ni * 8 + 2 * t;
+            double* dst = o + (size_t)r * b + n;
+            if (vec && n + 1 < wc) {
+              *reinterpret_cast<double2*>(dst) = make_double2(-acc[mi][ni][h * 2], -acc[mi][ni][h * 2 + 1]);
+            } else {
+              if (n < wc) dst[0] = -acc[mi][ni][h * 2];
+              if (n + 1 < wc) dst[1] = -acc[mi][ni][h * 2 + 1];
+            }
           }
-      }
+        }
+    }
     __syncthreads();  // the next step reads this tile and refills Ys
   }
 }
