@@ -49,6 +49,14 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
   return v;
 }
 
+// Relaxed load: a scan of several flags issues them back to back; a fence
+// afterwards gives the ones seen set acquire semantics.
+__device__ __forceinline__ int ld_relaxed(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }

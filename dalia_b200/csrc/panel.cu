@@ -197,9 +197,33 @@ __device__ bool acc_stream(const double* x, int xrows, const double* y, int yrow
   double* As = smem;
   double* Bs = smem + PST * PSLAB;
   bool ok = true;
+  // The leading source tiles whose producers have finished: one scan of
+  // their flags (relaxed loads in flight together, then one fence for
+  // acquire semantics) instead of a round trip per tile; later tiles are
+  // waited for one by one below.
+  __shared__ int s_ready;
+  if (gx != nullptr && tid == 0) {
+    const int nk = (kcols + T - 1) / T;
+    int r = 0;
+    bool run = true;
+    while (run && r < nk) {
+      int v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = (r + u < nk) ? min(ld_relaxed(gx + r + u), ld_relaxed(gy + r + u)) : 0;
+      int cnt = 0;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        if (run && v[u] >= 1) ++cnt;
+        else run = false;
+      }
+      r += cnt;
+    }
+    __threadfence();
+    s_ready = r;
+  }
   // issue slab j (after its gate, at the first slab of every tile)
   auto issue = [&](int j) {
-    if (gx != nullptr && ok && (j * PK) % T == 0) {
+    if (gx != nullptr && ok && (j * PK) % T == 0 && (j * PK) / T >= s_ready) {
       const int k = (j * PK) / T;
       if (tid == 0) *s_ok = (wait_ge(gx + k, 1, abort_flag) && wait_ge(gy + k, 1, abort_flag)) ? 1 : 0;
       __syncthreads();
